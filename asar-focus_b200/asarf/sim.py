@@ -1,0 +1,155 @@
+"""Seeded synthetic raw-data generator (test inputs; no public dataset exists for this path).
+
+A scene is circular complex Gaussian clutter plus a grid of point targets plus thermal
+noise, then the I/Q front-end impairments (DC bias, gain imbalance, quadrature skew) and
+quantisation to 5- or 8-bit offset-binary bytes, interleaved I,Q per sample as the ERS
+byte decoder expects.
+
+* point targets: exact hyperbolic range history R(eta) = sqrt(R0^2 + Vr^2 (eta-eta0)^2)
+  (so range migration is present), transmitted chirp exp(j pi Kr t^2), carrier phase
+  exp(-j 4 pi R / lambda), azimuth beam cos^2 centred on the Doppler centroid;
+* clutter: white reflectivity shaped in range by the chirp spectrum and in azimuth by the
+  same beam and the stationary-phase azimuth chirp, so its azimuth spectrum sits on the
+  Doppler centroid (which the ACCC estimator then measures).
+
+Runs on any torch device (the CUDA path only for speed on big scenes).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from .scene import SOL, Scene
+
+
+def _poly(p, x):
+    v = 0.0
+    for c in p:
+        v = v * x + c
+    return v
+
+
+def target_grid(sc: Scene) -> list[tuple[float, float]]:
+    """(range pixel, zero-Doppler azimuth line) of every point target."""
+    nk = sc.range_size - sc.chirp_samples
+    gx, gy = sc.grid
+    xs = np.linspace(0.15 * nk, 0.85 * nk, gx)
+    ys = np.linspace(0.3 * sc.azimuth_size, 0.7 * sc.azimuth_size, gy)
+    return [(float(round(x)) + 0.0, float(round(y)) + 0.0) for y in ys for x in xs]
+
+
+def simulate(sc: Scene, device: str | torch.device = "cpu", noise_rel: float = 0.25,
+             return_field: bool = False):
+    """Return (raw uint8 numpy [Na, 2*spl], truth dict)."""
+    dev = torch.device(device)
+    na, nr = sc.azimuth_size, sc.range_size
+    nc = sc.chirp_samples
+    fs = sc.range_sampling_rate
+    kr = sc.chirp_kr
+    prf = sc.prf
+    lam = sc.wavelength
+    dr = sc.range_spacing
+    vr_poly = sc.vr_poly if sc.vr_poly is not None else (0.0, 0.0, 7100.0)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(sc.seed))
+    cdt = torch.complex64
+    rdt = torch.float32
+
+    # ---------------------------------------------------------------- clutter
+    clut = torch.complex(torch.randn(na, nr, generator=gen, device=dev, dtype=rdt),
+                         torch.randn(na, nr, generator=gen, device=dev, dtype=rdt)) * (1 / math.sqrt(2))
+    n = torch.arange(nc, device=dev, dtype=torch.float64)
+    t = (n - nc // 2) / fs
+    chirp = torch.polar(torch.ones_like(t), math.pi * kr * t * t).to(cdt)
+    hr = torch.fft.fft(torch.nn.functional.pad(chirp, (0, nr - nc)))
+    clut = torch.fft.ifft(torch.fft.fft(clut, dim=1) * hr[None, :], dim=1)
+    # azimuth: per range column spectrum A(f - fdc) exp(j pi f^2 / Ka) * PRF / sqrt(Ka)
+    x = torch.arange(nr, device=dev, dtype=torch.float64)
+    r0 = sc.slant_range_first + x * dr
+    vr = _poly(vr_poly, x)
+    ka = 2 * vr * vr / (lam * r0)
+    fdc = torch.as_tensor(sc.dc_truth(np.arange(nr), na / 2), device=dev, dtype=torch.float64)
+    beam_bw = 0.95 * prf
+    spec = torch.fft.fft(clut, dim=0)
+    fb = torch.fft.fftfreq(na, d=1.0 / prf, device=dev).to(torch.float64)
+    chunk = max(1, (1 << 24) // na)
+    for c0 in range(0, nr, chunk):
+        c1 = min(nr, c0 + chunk)
+        f = fb[:, None] + torch.zeros(1, c1 - c0, device=dev, dtype=torch.float64)
+        d = fdc[None, c0:c1]
+        fa = f + prf * torch.round((d - f) / prf)          # unaliased Doppler within fdc +- prf/2
+        off = fa - d
+        beam = torch.where(off.abs() < beam_bw / 2, torch.cos(math.pi * off / beam_bw) ** 2,
+                           torch.zeros_like(off))
+        ph = torch.remainder(math.pi * fa * fa / ka[None, c0:c1], 2 * math.pi)
+        h = torch.polar(beam * (prf / torch.sqrt(ka[None, c0:c1])), ph)
+        spec[:, c0:c1] *= h.to(cdt)
+    clut = torch.fft.ifft(spec, dim=0)
+    del spec
+    clut_std = float(torch.sqrt(torch.mean(clut.real ** 2 + clut.imag ** 2) / 2))
+
+    # ---------------------------------------------------------------- point targets
+    field = clut
+    amp = 10 ** (sc.target_db / 20)
+    targets = target_grid(sc)
+    for (xt, yt) in targets:
+        r0t = sc.slant_range_first + xt * dr
+        vrt = _poly(vr_poly, xt)
+        kat = 2 * vrt * vrt / (lam * r0t)
+        fd = float(sc.dc_truth(np.array([xt]), yt)[0])
+        eta0 = yt / prf
+        etac = eta0 - fd / kat
+        half = beam_bw / (2 * kat)
+        y_lo = max(0, int(math.ceil((etac - half) * prf)))
+        y_hi = min(na - 1, int(math.floor((etac + half) * prf)))
+        if y_hi < y_lo:
+            continue
+        ys = torch.arange(y_lo, y_hi + 1, device=dev, dtype=torch.float64)
+        eta = ys / prf
+        rr = torch.sqrt(r0t * r0t + vrt * vrt * (eta - eta0) ** 2)
+        finst = -2 * vrt * vrt * (eta - eta0) / (lam * rr)
+        off = finst - fd
+        beam = torch.where(off.abs() < beam_bw / 2, torch.cos(math.pi * off / beam_bw) ** 2,
+                           torch.zeros_like(off))
+        p = (rr - sc.slant_range_first) / dr
+        i0 = torch.ceil(p)
+        k = torch.arange(nc, device=dev, dtype=torch.float64)
+        ii = i0[:, None] + k[None, :]
+        u = ii - p[:, None]
+        tt = (u - nc // 2) / fs
+        carrier = torch.remainder(-4 * math.pi * rr / lam, 2 * math.pi)
+        phase = torch.remainder(carrier[:, None] + math.pi * kr * tt * tt, 2 * math.pi)
+        val = torch.polar((amp * beam)[:, None].expand_as(phase), phase)
+        ok = (ii >= 0) & (ii < nr)
+        yy = ys[:, None].expand_as(ii).long()
+        field.index_put_((yy[ok], ii[ok].long()), val[ok].to(cdt), accumulate=True)
+
+    # ---------------------------------------------------------------- front end
+    bits = sc.bits
+    full = float(2 ** bits)
+    sigma_raw = 4.0 if bits == 5 else 30.0
+    scale = sigma_raw / max(clut_std, 1e-30)
+    z = field * scale
+    z = z + torch.complex(torch.randn(na, nr, generator=gen, device=dev, dtype=rdt),
+                          torch.randn(na, nr, generator=gen, device=dev, dtype=rdt)) * (noise_rel * sigma_raw)
+    skew = math.radians(sc.iq_skew_deg)
+    iv = z.real * sc.iq_gain
+    qv = z.imag * math.cos(skew) + z.real * math.sin(skew)
+    bias = full / 2 - 0.5
+    iq = torch.stack([iv + bias + sc.iq_bias[0], qv + bias + sc.iq_bias[1]], dim=-1)
+    iq = torch.clamp(torch.round(iq), 0, full - 1).to(torch.uint8)
+    if sc.swst_codes is not None:
+        sw = np.asarray(sc.swst_codes, dtype=np.int64)
+        offs = 4 * (sw - sw.min())
+        spl = sc.samples_per_line
+        out = torch.empty(na, spl, 2, dtype=torch.uint8, device=dev)
+        for y in range(na):
+            out[y] = iq[y, offs[y]:offs[y] + spl]
+        iq = out
+    raw = iq.reshape(na, -1).contiguous().cpu().numpy()
+    truth = dict(targets=targets, clutter_scale=scale, amp=amp)
+    if return_field:
+        truth["field"] = field
+    return raw, truth

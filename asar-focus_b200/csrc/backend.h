@@ -1,0 +1,38 @@
+// Execution backend of the planner: the CUDA kernels (kernels.cu, the product) or the
+// single-threaded host emulation of the same kernel bodies (emu.cpp, built only for the
+// CPU test suite as a separate library).
+#pragma once
+
+#include <cstddef>
+
+#include "params.h"
+
+namespace asarf {
+
+struct LaunchShape {
+    int threads;
+    size_t smem;
+};
+
+int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, int threads, int cols, void* stream);
+int backend_finalize(const FinalizeArgs& a, void* stream);
+int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void* stream);
+int backend_az_strided(const AzStridedArgs& a, int tiles, int nblocks, LaunchShape sh, void* stream);
+int backend_az_rd(const AzRdArgs& a, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void* stream);
+int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err, void* stream);
+
+void* mem_alloc(size_t bytes);
+void mem_free(void* p);
+int mem_h2d(void* dst, const void* src, size_t n, void* stream);
+int mem_d2h(void* dst, const void* src, size_t n, void* stream);
+int mem_d2d(void* dst, const void* src, size_t n, void* stream);
+int mem_d2d_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t rows, void* stream);
+int mem_zero(void* dst, size_t n, void* stream);
+int stream_sync(void* stream);
+size_t smem_optin_limit();
+const char* backend_name();
+
+// Records a message for asarf_last_error(); returns `code`.
+int set_error(int code, const char* fmt, ...);
+
+}  // namespace asarf

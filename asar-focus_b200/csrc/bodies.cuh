@@ -1,0 +1,584 @@
+// Kernel bodies of the focusing path, written once for the device and the host emulation.
+//
+// A body is a function of (block coordinates, tid, nthr, shared-memory pointer) made of
+// phases separated by ASARF_SYNC(); inside a phase every work item is independent.
+// Reference behaviour each body reproduces is cited in its comment
+// (paths relative to the asar-focus source tree).
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#include "fft.cuh"
+#include "hd.cuh"
+#include "params.h"
+
+namespace asarf {
+
+ASARF_HD ASARF_INLINE void atomic_or_u32(unsigned int* p, unsigned int v) {
+#if defined(__CUDA_ARCH__)
+    atomicOr(p, v);
+#else
+    *p |= v;
+#endif
+}
+
+// Device Polyval<N> of the reference (float Horner; nvcc contracts r*x + e into one fma).
+template <int N>
+ASARF_HD ASARF_INLINE float polyval_f32(const float (&p)[N], float x) {
+    float r = 0.0f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r = fma_rn(r, x, p[i]);
+    return r;
+}
+
+// ----------------------------------------------------------------------------- least squares
+// Householder-QR least-squares polynomial fit, coefficients highest power first
+// (Polyfit, util/src/math_utils.cc:23-44).  m <= 128 points, degree <= 4.
+template <int kM, int kN>
+ASARF_HD inline bool polyfit_qr(const double* x, const double* y, int m, int deg, double* out) {
+    const int n = deg + 1;
+    if (m > kM || n > kN || m < n) return false;
+    double A[kN][kM];  // column-major: A[col][row]
+    double b[kM];
+    for (int r = 0; r < m; ++r) {
+        double v = 1.0;
+        for (int c = 0; c < n; ++c) {
+            A[c][r] = v;
+            v *= x[r];
+        }
+        b[r] = y[r];
+    }
+    for (int k = 0; k < n; ++k) {
+        double nrm = 0.0;
+        for (int r = k; r < m; ++r) nrm += A[k][r] * A[k][r];
+        nrm = sqrt(nrm);
+        if (nrm == 0.0) return false;
+        const double alpha = A[k][k] > 0 ? -nrm : nrm;
+        // Householder vector v = A[k][k:] - alpha e_k kept in column k (its head in vk)
+        const double vk = A[k][k] - alpha;
+        double vn = vk * vk;
+        for (int r = k + 1; r < m; ++r) vn += A[k][r] * A[k][r];
+        if (vn == 0.0) return false;
+        for (int c = k + 1; c < n; ++c) {
+            double d = vk * A[c][k];
+            for (int r = k + 1; r < m; ++r) d += A[k][r] * A[c][r];
+            const double f = 2.0 * d / vn;
+            A[c][k] -= f * vk;
+            for (int r = k + 1; r < m; ++r) A[c][r] -= f * A[k][r];
+        }
+        double d = vk * b[k];
+        for (int r = k + 1; r < m; ++r) d += A[k][r] * b[r];
+        const double f = 2.0 * d / vn;
+        b[k] -= f * vk;
+        for (int r = k + 1; r < m; ++r) b[r] -= f * A[k][r];
+        A[k][k] = alpha;  // R diagonal
+    }
+    double c[kN];
+    for (int k = n - 1; k >= 0; --k) {
+        double s = b[k];
+        for (int j = k + 1; j < n; ++j) s -= A[j][k] * c[j];
+        c[k] = s / A[k][k];
+    }
+    for (int k = 0; k < n; ++k) out[k] = c[n - 1 - k];
+    return true;
+}
+
+// ----------------------------------------------------------------------------- raw statistics
+// One pass over the raw I/Q bytes.  Replaces, exactly and in integers, the reductions of
+// RawDataCorrection (sar/iq_correction.cu:188-274: mean, std-dev, gain and phase sums)
+// and of CalculateDopplerCentroid (sar/fractional_doppler_centroid.cu:33-69: lag-1
+// azimuth correlation per range block): the IQ correction is affine in the raw bytes,
+// so every sum the reference takes over corrected floats is a closed form of these.
+// Block (bx, by) covers columns [bx*cols, (bx+1)*cols) and lines [by*L, (by+1)*L).
+struct RawStatsSmem {
+    unsigned long long mom[6];
+    unsigned long long lag[kMaxDcBlocks][9];
+};
+
+ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by, int tid, int nthr, int cols,
+                                          RawStatsSmem* sm) {
+    unsigned long long* flat = &sm->mom[0];
+    const int nflat = 6 + a.nblk * 9;
+    for (int i = tid; i < 6 + kMaxDcBlocks * 9; i += nthr) flat[i] = 0ull;
+    ASARF_SYNC();
+    const int y0 = by * a.lines_per_cta;
+    const int y1 = (y0 + a.lines_per_cta < a.na) ? y0 + a.lines_per_cta : a.na;
+    const int ys = y0 > 0 ? y0 - 1 : 0;
+    for (int t = tid; t < cols; t += nthr) {
+        const int x = bx * cols + t;
+        const bool xin = x < a.nr;
+        unsigned long long cnt = 0, si = 0, sq = 0, sii = 0, sqq = 0, siq = 0;
+        unsigned int l[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        int pi = 0, pq = 0;
+        bool pf = false;
+        if (xin) {
+            for (int y = ys; y < y1; ++y) {
+                const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
+                const int i = x - off;
+                const bool f = (i >= 0) && (i < a.spl);
+                int iv = 0, qv = 0;
+                if (f) {
+                    const uint16_t w = *reinterpret_cast<const uint16_t*>(a.raw + static_cast<long long>(y) * a.line_bytes +
+                                                                          2ll * i);
+                    iv = w & 0xff;
+                    qv = w >> 8;
+                }
+                if (y >= y0) {
+                    if (f) {
+                        cnt += 1;
+                        si += iv;
+                        sq += qv;
+                        sii += iv * iv;
+                        sqq += qv * qv;
+                        siq += iv * qv;
+                    }
+                    if (y > 0 && f && pf) {
+                        l[0] += 1;
+                        l[1] += pi;
+                        l[2] += pq;
+                        l[3] += iv;
+                        l[4] += qv;
+                        l[5] += pi * iv;
+                        l[6] += pq * qv;
+                        l[7] += pi * qv;
+                        l[8] += pq * iv;
+                    }
+                }
+                pi = iv;
+                pq = qv;
+                pf = f;
+            }
+        }
+        unsigned long long mv[6] = {cnt, si, sq, sii, sqq, siq};
+        const int blk = xin ? x / a.dc_step : 0;
+#if defined(__CUDA_ARCH__)
+        // warp reduction first: all lanes run this loop iteration (cols is a multiple of nthr)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            unsigned long long v = mv[k];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            mv[k] = v;
+        }
+        if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
+        }
+        const int bmin = __reduce_min_sync(0xffffffffu, xin ? blk : 0x7fffffff);
+        const int bmax = __reduce_max_sync(0xffffffffu, xin ? blk : -1);
+        if (bmin == bmax) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                unsigned int v = xin ? l[k] : 0u;
+                v = __reduce_add_sync(0xffffffffu, v);
+                l[k] = v;
+            }
+            if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) atomic_add_u64(&sm->lag[bmin][k], l[k]);
+            }
+        } else if (xin) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) atomic_add_u64(&sm->lag[blk][k], l[k]);
+        }
+#else
+        for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
+        if (xin)
+            for (int k = 0; k < 9; ++k) atomic_add_u64(&sm->lag[blk][k], l[k]);
+#endif
+    }
+    ASARF_SYNC();
+    unsigned long long* gflat = &a.acc->mom[0];
+    for (int i = tid; i < nflat; i += nthr) {
+        const unsigned long long v = flat[i];
+        if (v) atomic_add_u64(gflat + i, v);
+    }
+}
+
+// ----------------------------------------------------------------------------- finalisation
+// Single-threaded: IQ statistics and correction constants exactly as RawDataCorrection
+// derives them (sar/iq_correction.cu:200-273, CalcMean/CalcStdDev of
+// cuda_util/device_padded_image.cu:331-414), the Doppler centroid per range block and its
+// quadratic fit (sar/fractional_doppler_centroid.cu:98-139), and the results-window choice
+// that depends on the sign of the fitted constant term (main_flow.cc:155-178).
+ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
+    const StatAccum& s = *a.acc;
+    FocusState& st = *a.state;
+    const double n = static_cast<double>(s.mom[0]);
+    const double SI = static_cast<double>(s.mom[1]), SQ = static_cast<double>(s.mom[2]);
+    const double SII = static_cast<double>(s.mom[3]), SQQ = static_cast<double>(s.mom[4]);
+    const double SIQ = static_cast<double>(s.mom[5]);
+    unsigned int err = 0;
+    if (s.mom[0] == 0) err |= kErrStatsEmpty;
+    const float total = static_cast<float>(a.n_total);
+    // mean: float(sum) / float(total)
+    const float dc_i = static_cast<float>(SI) / total;
+    const float dc_q = static_cast<float>(SQ) / total;
+    const double di = dc_i, dq = dc_q;
+    const double cii = SII - 2.0 * di * SI + n * di * di;  // sum over filled of (I - dc_i)^2
+    const double cqq = SQQ - 2.0 * dq * SQ + n * dq * dq;
+    const double ciq = SIQ - dq * SI - di * SQ + n * di * dq;
+    const float std_i = sqrtf(static_cast<float>(cii) / total);
+    const float std_q = sqrtf(static_cast<float>(cqq) / total);
+    // padding samples hold 0 - dc after the DC step and enter the gain / phase sums
+    const double npad = static_cast<double>(a.n_pad);
+    const double i1sq = cii + npad * di * di;
+    const double q1sq = cqq + npad * dq * dq;
+    const double i1q1 = ciq + npad * di * dq;
+    const double gain = sqrt(i1sq / q1sq);
+    const float gain_f = static_cast<float>(gain);
+    const double gf = gain_f;
+    const double delta = (i1q1 / gf) / (i1sq / (gf * gf));
+    const float sin_c = static_cast<float>(delta);
+    const float cos_c = static_cast<float>(1.0 - delta * delta);
+    st.dc_i = dc_i;
+    st.dc_q = dc_q;
+    st.gain = gain_f;
+    st.sin_c = sin_c;
+    st.cos_c = cos_c;
+    st.dc_i_d = dc_i;
+    st.dc_q_d = dc_q;
+    st.iq_gain = gain;
+    st.phase_error = 360.0 * asin(delta) / (2.0 * 3.14159265358979323846);
+    st.stddev_i = std_i;
+    st.stddev_q = std_q;
+
+    // corrected sample z = (p*I + p0, u*Q + v*I + w)
+    const double p = 1.0 / gf, p0 = -di / gf;
+    const double sc = sin_c, cc = cos_c;
+    const double u = 1.0 / cc, v = -sc * p / cc, w = (-dq - sc * p0) / cc;
+    const double pad_mag2 = p0 * p0 + w * w;  // |corrected zero padding sample|^2
+    double xs[kMaxDcBlocks], ys[kMaxDcBlocks];
+    const int nblk = a.nblk < kMaxDcBlocks ? a.nblk : kMaxDcBlocks;
+    if (a.nblk > kMaxDcBlocks) err |= kErrDcBlocks;
+    for (int b = 0; b < nblk; ++b) {
+        const unsigned long long* L = s.lag[b];
+        const double np = static_cast<double>(L[0]);
+        const double sA = static_cast<double>(L[1]), sB = static_cast<double>(L[2]);
+        const double sC = static_cast<double>(L[3]), sD = static_cast<double>(L[4]);
+        const double sAC = static_cast<double>(L[5]), sBD = static_cast<double>(L[6]);
+        const double sAD = static_cast<double>(L[7]), sBC = static_cast<double>(L[8]);
+        double re = p * p * sAC + p * p0 * (sA + sC) + p0 * p0 * np + u * u * sBD + u * v * (sBC + sAD) +
+                    u * w * (sB + sD) + v * v * sAC + v * w * (sA + sC) + w * w * np;
+        const double im = p * u * (sAD - sBC) + p * w * (sA - sC) + p0 * u * (sD - sB) + p0 * v * (sC - sA);
+        const int xb = b * a.dc_step;
+        const int xe = xb + a.dc_step;
+        // columns of this block beyond the data lie in the range padding (constant rows)
+        int pad_lo = xb > a.nr ? xb : a.nr;
+        int pad_hi = xe < a.rg_stride ? xe : a.rg_stride;
+        if (pad_hi > pad_lo) re += static_cast<double>(pad_hi - pad_lo) * (a.na - 1) * pad_mag2;
+        const double ang = atan2(im, re);
+        const double hz = a.prf * (ang / (2.0 * 3.14159265358979323846));
+        xs[b] = static_cast<double>((xb + xe) / 2);
+        ys[b] = hz;
+        st.dc_blk_hz[b] = hz;
+    }
+    st.nblk = nblk;
+    double poly[3] = {0.0, 0.0, 0.0};
+    polyfit_qr<kMaxDcBlocks, 3>(xs, ys, nblk, 2, poly);
+    for (int k = 0; k < 3; ++k) {
+        st.dc_poly[k] = poly[k];
+        st.dc_poly32[k] = static_cast<float>(poly[k]);
+    }
+    st.variant = poly[2] > 0 ? 0 : 1;
+    st.first_line = a.first_line[st.variant];
+    st.n_lines = a.n_lines[st.variant];
+    st.errors = err;
+}
+
+// ----------------------------------------------------------------------------- range compression
+// One azimuth line per block: ERS byte decode (envisat_format/src/envisat_format_kernels.cu:116-134),
+// IQ correction with the reference's float operation order (sar/iq_correction.cu:140-178),
+// forward FFT, chirp matched filter and inverse FFT (sar/range_compression.cu:25-107), keeping
+// x < XSize - chirp_samples.  Samples the decoder leaves empty are 0 (ZeroNaNs after the
+// correction, main.cc:245).  The FFT length is any L >= XSize: outputs x < Nk only correlate
+// data samples [x, x + Nc) so they do not depend on L.
+ASARF_HD ASARF_INLINE float2 correct_sample(int iv, int qv, const FocusState& st) {
+    const float i1 = fsub_rn(static_cast<float>(iv), st.dc_i);
+    const float q1 = fsub_rn(static_cast<float>(qv), st.dc_q);
+    const float i2 = fdiv_rn(i1, st.gain);
+    const float q2 = fdiv_rn(fma_rn(-i2, st.sin_c, q1), st.cos_c);
+    return make_float2(i2, q2);
+}
+
+ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y, int tid, int nthr, float2* s) {
+    const FocusState& st = *a.state;
+    const int L = a.plan.n;
+    const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
+    const uint8_t* row = a.raw + static_cast<long long>(y) * a.line_bytes;
+    for (int l = tid; l < L; l += nthr) {
+        float2 z = make_float2(0.0f, 0.0f);
+        const int i = l - off;
+        if (l < a.nr && i >= 0 && i < a.spl) {
+            const uint16_t wv = *reinterpret_cast<const uint16_t*>(row + 2ll * i);
+            z = correct_sample(wv & 0xff, wv >> 8, st);
+        }
+        s[l] = z;
+    }
+    ASARF_SYNC();
+    fft_forward(a.plan, s, 1, 1, tid, nthr);
+    for (int l = tid; l < L; l += nthr) s[l] = cmul(s[l], ASARF_LDG(a.mf + l));
+    ASARF_SYNC();
+    fft_inverse(a.plan, s, 1, 1, tid, nthr);
+    float2* orow = a.out + static_cast<long long>(y) * a.out_pitch;
+    for (int l = tid; l < a.nk; l += nthr) orow[l] = s[l];
+}
+
+// ----------------------------------------------------------------------------- azimuth strided pass
+// Four-step azimuth FFT of length N = n1 * n2 along the rows of a [N][pitch] block, columns
+// [x0, x0 + xt).  Time index n = a*n2 + b, frequency k = k1 + n1*k2.
+//  forward (block b): Y[k1][b] = W_N^{b k1} * FFT_n1(x[a*n2 + b])[k1], stored at row k1*n2 + b.
+//  inverse (block b): x[a*n2 + b] = IFFT_n1(conj(W_N^{b k1}) * Z[k1][b])[a] * scale.
+// Together with the contiguous pass this is the transpose-free equivalent of the reference's
+// transpose + batched row FFT + transpose (sar/range_doppler_algorithm.cu:314-326, 381-391).
+ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int b, int tid, int nthr, float2* s) {
+    const int x0 = tile * a.xt;
+    const int n1 = a.n1, xt = a.xt;
+    if (!a.inverse) {
+        for (int t = tid; t < n1 * xt; t += nthr) {
+            const int r = t / xt, c = t - r * xt;
+            const int row = r * a.n2 + b;
+            const int x = x0 + c;
+            float2 v = make_float2(0.0f, 0.0f);
+            if (row < a.valid_rows && x < a.nk) v = a.in[static_cast<long long>(row) * a.pitch + x];
+            s[t] = v;
+        }
+        ASARF_SYNC();
+        fft_forward(a.plan1, s, xt, xt, tid, nthr);
+        for (int t = tid; t < n1 * xt; t += nthr) {
+            const int p = t / xt, c = t - p * xt;
+            const int k1 = ASARF_LDG(a.drev1 + p);
+            const int x = x0 + c;
+            if (x < a.nk) {
+                const float2 tw = ASARF_LDG(a.twn + b * k1);
+                a.out[static_cast<long long>(k1 * a.n2 + b) * a.pitch + x] = cmul(s[t], tw);
+            }
+        }
+    } else {
+        const int lo = a.state ? a.state->first_line : 0;
+        const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
+        for (int t = tid; t < n1 * xt; t += nthr) {
+            const int p = t / xt, c = t - p * xt;
+            const int k1 = ASARF_LDG(a.drev1 + p);
+            const int x = x0 + c;
+            float2 v = make_float2(0.0f, 0.0f);
+            if (x < a.nk) {
+                v = a.in[static_cast<long long>(k1 * a.n2 + b) * a.pitch + x];
+                v = cmulc(v, ASARF_LDG(a.twn + b * k1));
+            }
+            s[t] = v;
+        }
+        ASARF_SYNC();
+        fft_inverse(a.plan1, s, xt, xt, tid, nthr);
+        for (int t = tid; t < n1 * xt; t += nthr) {
+            const int r = t / xt, c = t - r * xt;
+            const int row = r * a.n2 + b;
+            const int x = x0 + c;
+            if (x < a.nk && row >= lo && row < hi) {
+                const float2 v = s[t];
+                a.out[static_cast<long long>(row) * a.pitch + x] = make_float2(fmul_rn(v.x, a.scale), fmul_rn(v.y, a.scale));
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------- range-Doppler block
+// Block (tile, k1): rows k1*n2 .. k1*n2 + n2 - 1 of the strided-pass output, output columns
+// [x0, x0 + xt) plus a range halo (hl left, hr right) for the interpolator.
+//   1. contiguous forward FFT_n2 -> range-Doppler rows, frequency bin k1 + n1*drev2(p);
+//   2. RCMC: 16-tap Blackman-windowed sinc at the parabolic range walk
+//      (RangeCellMigrationCorrection, sar/range_doppler_algorithm.cu:107-195);
+//   3. azimuth matched filter with Doppler-centroid band cut and linear phase ramp
+//      (AzimuthReferenceMultiply, sar/range_doppler_algorithm.cu:197-309);
+//   4. contiguous inverse FFT_n2 of the xt output columns.
+// Both use the reference's float32 operation order for every branch-deciding quantity.
+ASARF_HD ASARF_INLINE ColParams az_col_params(const AzRdArgs& a, int x) {
+    ColParams cp;
+    const float xf = static_cast<float>(x);
+    float dcp[3] = {a.state->dc_poly32[0], a.state->dc_poly32[1], a.state->dc_poly32[2]};
+    float vrp[3] = {a.vr_poly[0], a.vr_poly[1], a.vr_poly[2]};
+    cp.dc = polyval_f32(dcp, xf);
+    cp.vr = polyval_f32(vrp, xf);
+    const float step = fdiv_rn(a.prf, static_cast<float>(a.az_pad));
+    const float dc_steps = roundf(fdiv_rn(cp.dc, step));
+    cp.dc_off = fmul_rn(dc_steps, step);
+    cp.r0 = a.slant + static_cast<double>(x) * a.range_spacing;
+    const float kav = fmul_rn(fmul_rn(2.0f, cp.vr), cp.vr);
+    cp.ka = static_cast<float>(static_cast<double>(kav) / (static_cast<double>(a.lambda) * cp.r0));
+    const float half = fmul_rn(a.prf, 0.5f);
+    cp.cut_hi = fma_rn(half, a.frac, cp.dc_off);
+    cp.cut_lo = fma_rn(-half, a.frac, cp.dc_off);
+    return cp;
+}
+
+ASARF_HD ASARF_INLINE float bin_frequency(int f, int az_pad, float step) {
+    const int k = (f < az_pad / 2) ? f : f - az_pad;
+    return fmul_rn(static_cast<float>(k), step);
+}
+
+ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& cp, int x, int f, const float2* srow,
+                                            int cs, unsigned int* err_flag) {
+    const float prf = a.prf;
+    const float step = fdiv_rn(prf, static_cast<float>(a.az_pad));
+    const float half = fmul_rn(prf, 0.5f);
+    const float bf = bin_frequency(f, a.az_pad, step);
+    // --- RCMC (aliased frequency, range walk)
+    float fn = bf;
+    if (cp.dc < 0.0f) {
+        if (fn > fadd_rn(half, cp.dc)) fn = fsub_rn(fn, prf);
+    } else if (cp.dc > 0.0f) {
+        if (fn < fadd_rn(-half, cp.dc)) fn = fadd_rn(fn, prf);
+    }
+    const float num = fmul_rn(fmul_rn(fmul_rn(a.lambda, a.lambda), fn), fn);
+    const float den = fmul_rn(fmul_rn(8.0f, cp.vr), cp.vr);
+    double dr = static_cast<double>(fdiv_rn(num, den));
+    dr *= cp.r0;
+    const float shift = static_cast<float>(dr / a.range_spacing);
+    const int walk = static_cast<int>(roundf(shift));
+    const int calc_x = x + walk;
+    float2 out = make_float2(0.0f, 0.0f);
+    if (!(calc_x - kRcmcTaps / 2 < 0 || calc_x + kRcmcTaps / 2 >= a.nk)) {
+        const int first = cs + walk - kRcmcTaps / 2;  // smem column of tap 0
+        if (first < 0 || first + kRcmcTaps > a.wt) {
+            atomic_or_u32(err_flag, kErrRcmcHalo);
+        } else {
+            const float off = fadd_rn(fsub_rn(shift, static_cast<float>(walk)), static_cast<float>(kRcmcTaps / 2));
+            const float pi = 3.14159265358979323846f;
+            float si = 0.0f, sq = 0.0f, nrm = 0.0f;
+#pragma unroll
+            for (int i = 0; i < kRcmcTaps; ++i) {
+                const float arg = fsub_rn(off, static_cast<float>(i));
+                float sinc = 1.0f;
+                if (arg != 0.0f) {
+                    const float pa = fmul_rn(pi, arg);
+                    sinc = fdiv_rn(sinf(pa), pa);
+                }
+                const float wgt = fmul_rn(ASARF_LDG(a.win + i), sinc);
+                const float2 d = srow[first + i];
+                si = fma_rn(d.x, wgt, si);
+                sq = fma_rn(d.y, wgt, sq);
+                nrm = fadd_rn(nrm, wgt);
+            }
+            if (nrm != 0.0f) out = make_float2(fdiv_rn(si, nrm), fdiv_rn(sq, nrm));
+        }
+    }
+    // --- azimuth matched filter
+    float absf = bf;
+    if (cp.dc < 0.0f) {
+        if (bf > fadd_rn(half, cp.dc)) absf = fsub_rn(absf, prf);
+    } else if (cp.dc > 0.0f) {
+        if (absf < fadd_rn(-half, cp.dc)) absf = fadd_rn(absf, prf);
+    }
+    if (absf < cp.cut_lo || absf > cp.cut_hi) return make_float2(0.0f, 0.0f);
+    float fc = fsub_rn(bf, cp.dc_off);
+    if (fc > half) fc = fsub_rn(fc, prf);
+    else if (fc < -half) fc = fadd_rn(fc, prf);
+    const float pi = 3.14159265358979323846f;
+    const float mf_phase = fdiv_rn(fmul_rn(fmul_rn(pi, fc), fc), cp.ka);
+    float s1, c1, s2, c2;
+    sincosf(mf_phase, &s1, &c1);
+    const float sh_phase = fmul_rn(fmul_rn(fmul_rn(2.0f, pi), fdiv_rn(cp.dc_off, cp.ka)), bf);
+    sincosf(sh_phase, &s2, &c2);
+    const float2 mf = cmul(make_float2(c1, -s1), make_float2(c2, -s2));
+    return cmul(out, mf);
+}
+
+ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s, float2* tmp,
+                                      ColParams* cps, unsigned int* err_flag) {
+    const int x0 = tile * a.xt;
+    const int n2 = a.n2, wt = a.wt;
+    for (int t = tid; t < n2 * wt; t += nthr) {
+        const int r = t / wt, c = t - r * wt;
+        const int x = x0 - a.hl + c;
+        float2 v = make_float2(0.0f, 0.0f);
+        if (x >= 0 && x < a.nk) v = a.in[static_cast<long long>(k1 * n2 + r) * a.pitch + x];
+        s[t] = v;
+    }
+    for (int c = tid; c < a.xt; c += nthr) cps[c] = az_col_params(a, x0 + c);
+    ASARF_SYNC();
+    fft_forward(a.plan2, s, wt, wt, tid, nthr);
+    // RCMC + matched filter, chunk_rows rows at a time through tmp (in-place safe)
+    for (int r0 = 0; r0 < n2; r0 += a.chunk_rows) {
+        const int rn = (r0 + a.chunk_rows < n2) ? a.chunk_rows : n2 - r0;
+        for (int t = tid; t < rn * a.xt; t += nthr) {
+            const int rr = t / a.xt, c = t - rr * a.xt;
+            const int p = r0 + rr;
+            const int x = x0 + c;
+            float2 v = make_float2(0.0f, 0.0f);
+            if (x < a.nk) {
+                const int f = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
+                v = rcmc_mf_sample(a, cps[c], x, f, s + p * wt, a.hl + c, err_flag);
+            }
+            tmp[t] = v;
+        }
+        ASARF_SYNC();
+        for (int t = tid; t < rn * a.xt; t += nthr) {
+            const int rr = t / a.xt, c = t - rr * a.xt;
+            s[(r0 + rr) * wt + a.hl + c] = tmp[t];
+        }
+        ASARF_SYNC();
+    }
+    fft_inverse(a.plan2, s + a.hl, a.xt, wt, tid, nthr);
+    for (int t = tid; t < n2 * a.xt; t += nthr) {
+        const int r = t / a.xt, c = t - r * a.xt;
+        const int x = x0 + c;
+        if (x < a.nk) a.out[static_cast<long long>(k1 * n2 + r) * a.pitch + x] = s[r * wt + a.hl + c];
+    }
+}
+
+// ----------------------------------------------------------------------------- detected tail
+// One output line per block: results-window subset (main_flow.cc:585-627), time-domain
+// azimuth multilook (TimeDomainAzimuthLook, sar/az_multilook.cu:25-80), range spreading loss
+// gain (sar/range_spreading_loss.cu:29-52) and slant-to-ground resampling with the
+// reference's float Horner / IEEE division / truncation index (SrGrInterpolation,
+// sar/srgr.cu:49-71).  ml holds one multilooked slant row (nx floats).
+ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr, float* ml, unsigned int* err_flag) {
+    const FocusState& st = *a.state;
+    const TailVariant& tv = a.tail[st.variant];
+    if (y >= tv.out_az) return;
+    const int in_y = st.n_lines;
+    const float in_idx = fmul_rn(static_cast<float>(y), tv.ratio);
+    const float mu = fsub_rn(in_idx, static_cast<float>(static_cast<int>(in_idx)));
+    int s0 = static_cast<int>(fsub_rn(in_idx, 2.0f)), e0 = static_cast<int>(fadd_rn(in_idx, 2.0f));
+    int s1 = static_cast<int>(fsub_rn(in_idx, 1.0f)), e1 = static_cast<int>(fadd_rn(in_idx, 3.0f));
+    s0 = s0 > 0 ? s0 : 0;
+    s1 = s1 > 0 ? s1 : 0;
+    e0 = e0 < in_y ? e0 : in_y;
+    e1 = e1 < in_y ? e1 : in_y;
+    const int c0 = e0 > s0 ? e0 - s0 : 0;
+    const int c1 = e1 > s1 ? e1 - s1 : 0;
+    const float2* base = a.slc + static_cast<long long>(st.first_line) * a.pitch + a.col0;
+    for (int c = tid; c < a.nx; c += nthr) {
+        float sum0 = 0.0f, sum1 = 0.0f;
+        for (int r = s0; r < e0; ++r) {
+            const float2 v = base[static_cast<long long>(r) * a.pitch + c];
+            sum0 = fadd_rn(sum0, fma_rn(v.x, v.x, fmul_rn(v.y, v.y)));
+        }
+        for (int r = s1; r < e1; ++r) {
+            const float2 v = base[static_cast<long long>(r) * a.pitch + c];
+            sum1 = fadd_rn(sum1, fma_rn(v.x, v.x, fmul_rn(v.y, v.y)));
+        }
+        if (c0) sum0 = fdiv_rn(sum0, static_cast<float>(c0));
+        if (c1) sum1 = fdiv_rn(sum1, static_cast<float>(c1));
+        float val = 0.0f;
+        if (c0 && c1) val = fma_rn(fsub_rn(sum1, sum0), mu, sum0);
+        ml[c] = fmul_rn(val, ASARF_LDG(tv.rsl + c));
+    }
+    ASARF_SYNC();
+    float* orow = a.out + static_cast<long long>(y) * a.out_pitch;
+    for (int xg = tid; xg < tv.ng; xg += nthr) {
+        const float gd = fmul_rn(static_cast<float>(xg), a.ground_spacing);
+        const float rd = polyval_f32(tv.grsr, gd);
+        const float idx = fdiv_rn(rd, a.range_spacing);
+        int i0 = static_cast<int>(idx);
+        const float dx = fsub_rn(idx, static_cast<float>(i0));
+        if (i0 < 0 || i0 + 1 >= a.nx) {
+            atomic_or_u32(err_flag, kErrSrgrIndex);
+            i0 = i0 < 0 ? 0 : a.nx - 2;
+        }
+        const float v0 = ml[i0], v1 = ml[i0 + 1];
+        orow[xg] = fma_rn(dx, fsub_rn(v1, v0), v0);
+    }
+}
+
+}  // namespace asarf

@@ -1,0 +1,237 @@
+// Shared-memory mixed-radix FFT building blocks for sm_100a.
+//
+// Every transform here works IN PLACE on a tile held in shared memory, laid out as
+// element (l, c) at s[l * ldc + c]: l in [0, n) runs along the transform, c in [0, ncol)
+// indexes independent transforms (range lines, or range columns of an azimuth block).
+//
+//  * forward transforms are decimation-in-frequency: natural-order input, digit-reversed
+//    output (position p holds frequency digit_reverse(p));
+//  * inverse transforms are decimation-in-time: digit-reversed input, natural-order
+//    output, unscaled.
+//
+// Pairing the two removes every reordering pass: a frequency-domain operation (chirp
+// matched filter, RCMC, azimuth matched filter) only needs to know which frequency each
+// position holds.  Radices 2, 3, 4, 5, 7 and 8 cover all 2^a 3^b 5^c 7^d lengths the
+// range / azimuth padding rules produce.  Twiddles come from a per-length table
+// tw[m] = exp(-2*pi*i*m/n), m in [0, n), computed in FP64 on the host.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "hd.cuh"
+
+namespace asarf {
+
+constexpr int kMaxStages = 16;
+
+// Radix schedule of one transform length (host-built, passed by value to kernels).
+struct FftPlan {
+    int n;
+    int nst;
+    int radix[kMaxStages];
+    int span[kMaxStages];  // S of stage i (block length M = S * radix)
+    const float2* tw;      // n entries
+};
+
+ASARF_HD ASARF_INLINE float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+ASARF_HD ASARF_INLINE float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+ASARF_HD ASARF_INLINE float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+ASARF_HD ASARF_INLINE float2 cmulc(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+ASARF_HD ASARF_INLINE float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+ASARF_HD ASARF_INLINE float2 mul_mi(float2 a) {
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// ----------------------------------------------------------------------------- small DFTs
+// Sign convention: forward y_k = sum_m x_m exp(-2 pi i m k / R), inverse uses +.
+
+template <bool INV>
+ASARF_HD ASARF_INLINE void dft2(float2* v) {
+    float2 a = v[0];
+    v[0] = cadd(a, v[1]);
+    v[1] = csub(a, v[1]);
+}
+
+template <bool INV>
+ASARF_HD ASARF_INLINE void dft4(float2* v) {
+    float2 t0 = cadd(v[0], v[2]);
+    float2 t1 = csub(v[0], v[2]);
+    float2 t2 = cadd(v[1], v[3]);
+    float2 t3 = mul_mi<INV>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+}
+
+template <bool INV>
+ASARF_HD ASARF_INLINE void dft8(float2* v) {
+    constexpr float h = 0.7071067811865476f;
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<INV>(e);
+    dft4<INV>(o);
+    // o_k *= W8^k (forward W8 = exp(-i pi/4))
+    float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                    : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    float2 o2 = mul_mi<INV>(o[2]);
+    float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                    : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+}
+
+template <bool INV>
+ASARF_HD ASARF_INLINE void dft3(float2* v) {
+    constexpr float s3 = 0.8660254037844387f;
+    float2 a = cadd(v[1], v[2]);
+    float2 b = csub(v[1], v[2]);
+    float2 t = make_float2(v[0].x - 0.5f * a.x, v[0].y - 0.5f * a.y);
+    float2 u = mul_mi<INV>(cscale(b, s3));
+    v[0] = cadd(v[0], a);
+    v[1] = cadd(t, u);
+    v[2] = csub(t, u);
+}
+
+template <bool INV>
+ASARF_HD ASARF_INLINE void dft5(float2* v) {
+    constexpr float c1 = 0.30901699437494745f, s1 = 0.9510565162951535f;
+    constexpr float c2 = -0.8090169943749473f, s2 = 0.5877852522924732f;
+    float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    float2 x0 = v[0];
+    float2 r1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+    float2 r2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+    float2 i1 = mul_mi<INV>(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
+    float2 i2 = mul_mi<INV>(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
+    v[0] = make_float2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+    v[1] = cadd(r1, i1);
+    v[4] = csub(r1, i1);
+    v[2] = cadd(r2, i2);
+    v[3] = csub(r2, i2);
+}
+
+template <bool INV>
+ASARF_HD ASARF_INLINE void dft7(float2* v) {
+    constexpr float c1 = 0.6234898018587336f, s1 = 0.7818314824680298f;
+    constexpr float c2 = -0.22252093395631434f, s2 = 0.9749279121818236f;
+    constexpr float c3 = -0.900968867902419f, s3 = 0.43388373911755823f;
+    float2 a1 = cadd(v[1], v[6]), b1 = csub(v[1], v[6]);
+    float2 a2 = cadd(v[2], v[5]), b2 = csub(v[2], v[5]);
+    float2 a3 = cadd(v[3], v[4]), b3 = csub(v[3], v[4]);
+    float2 x0 = v[0];
+    // k = 1..3: cos(2 pi m k / 7) pattern over m = 1..3; sin pattern with sign folding
+    float2 r1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x + c3 * a3.x, x0.y + c1 * a1.y + c2 * a2.y + c3 * a3.y);
+    float2 r2 = make_float2(x0.x + c2 * a1.x + c3 * a2.x + c1 * a3.x, x0.y + c2 * a1.y + c3 * a2.y + c1 * a3.y);
+    float2 r3 = make_float2(x0.x + c3 * a1.x + c1 * a2.x + c2 * a3.x, x0.y + c3 * a1.y + c1 * a2.y + c2 * a3.y);
+    // sin(2 pi m k / 7): k=1: s1 s2 s3 ; k=2: s2 -s3 -s1 ; k=3: s3 -s1 s2
+    float2 i1 = mul_mi<INV>(make_float2(s1 * b1.x + s2 * b2.x + s3 * b3.x, s1 * b1.y + s2 * b2.y + s3 * b3.y));
+    float2 i2 = mul_mi<INV>(make_float2(s2 * b1.x - s3 * b2.x - s1 * b3.x, s2 * b1.y - s3 * b2.y - s1 * b3.y));
+    float2 i3 = mul_mi<INV>(make_float2(s3 * b1.x - s1 * b2.x + s2 * b3.x, s3 * b1.y - s1 * b2.y + s2 * b3.y));
+    v[0] = make_float2(x0.x + a1.x + a2.x + a3.x, x0.y + a1.y + a2.y + a3.y);
+    v[1] = cadd(r1, i1);
+    v[6] = csub(r1, i1);
+    v[2] = cadd(r2, i2);
+    v[5] = csub(r2, i2);
+    v[3] = cadd(r3, i3);
+    v[4] = csub(r3, i3);
+}
+
+template <int R, bool INV>
+ASARF_HD ASARF_INLINE void dft(float2* v) {
+    if constexpr (R == 2) dft2<INV>(v);
+    else if constexpr (R == 3) dft3<INV>(v);
+    else if constexpr (R == 4) dft4<INV>(v);
+    else if constexpr (R == 5) dft5<INV>(v);
+    else if constexpr (R == 7) dft7<INV>(v);
+    else if constexpr (R == 8) dft8<INV>(v);
+}
+
+// ----------------------------------------------------------------------------- one stage
+// Butterfly item t -> (column c = t % ncol, butterfly bj = t / ncol); bj -> (block b, offset j).
+// Forward (DIF): load R values at stride S, small DFT, multiply output q by W_M^{j q}.
+// Inverse (DIT): multiply input q by conj(W_M^{j q}), small inverse DFT.
+template <int R, bool INV>
+ASARF_HD ASARF_INLINE void fft_stage(float2* s, int n, int S, int ncol, int ldc, const float2* __restrict__ tw,
+                                          int tid, int nthr) {
+    const int M = S * R;
+    const int items = (n / R) * ncol;
+    const int tw_step = n / M;
+    for (int t = tid; t < items; t += nthr) {
+        int c, bj;
+        if (ncol == 1) {
+            c = 0;
+            bj = t;
+        } else {
+            bj = t / ncol;
+            c = t - bj * ncol;
+        }
+        const int b = bj / S;
+        const int j = bj - b * S;
+        float2* p = s + (b * M + j) * ldc + c;
+        const int st = S * ldc;
+        float2 v[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[m] = p[m * st];
+        if (INV) {
+            if (j != 0) {
+#pragma unroll
+                for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], ASARF_LDG(tw + j * q * tw_step));
+            }
+            dft<R, true>(v);
+        } else {
+            dft<R, false>(v);
+            if (j != 0) {
+#pragma unroll
+                for (int q = 1; q < R; ++q) v[q] = cmul(v[q], ASARF_LDG(tw + j * q * tw_step));
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) p[m * st] = v[m];
+    }
+}
+
+template <bool INV>
+ASARF_HD ASARF_INLINE void fft_stage_dispatch(int R, float2* s, int n, int S, int ncol, int ldc,
+                                                   const float2* __restrict__ tw, int tid, int nthr) {
+    switch (R) {
+        case 2: fft_stage<2, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
+        case 3: fft_stage<3, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
+        case 4: fft_stage<4, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
+        case 5: fft_stage<5, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
+        case 7: fft_stage<7, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
+        default: fft_stage<8, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
+    }
+}
+
+// Forward DIF transform of ncol independent columns; output digit-reversed.  The caller
+// places a barrier after loading the tile; this returns after a final barrier.
+ASARF_HD ASARF_INLINE void fft_forward(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    for (int i = 0; i < p.nst; ++i) {
+        fft_stage_dispatch<false>(p.radix[i], s, p.n, p.span[i], ncol, ldc, p.tw, tid, nthr);
+        ASARF_SYNC();
+    }
+}
+
+// Inverse DIT transform (digit-reversed input, natural output, unscaled).
+ASARF_HD ASARF_INLINE void fft_inverse(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    for (int i = p.nst - 1; i >= 0; --i) {
+        fft_stage_dispatch<true>(p.radix[i], s, p.n, p.span[i], ncol, ldc, p.tw, tid, nthr);
+        ASARF_SYNC();
+    }
+}
+
+}  // namespace asarf

@@ -1,0 +1,88 @@
+// Host/device portability macros for the kernel bodies.
+//
+// Every kernel in this library is written as a sequence of barrier-separated phases in
+// which thread `tid` of `nthr` walks a strided loop over independent work items.  The
+// device build runs the phases with real threads and __syncthreads() between them.  The
+// host-emulation build (ASARF_HOST_EMU, used only by the CPU test suite) runs the same
+// code with tid = 0, nthr = 1, so a barrier is a no-op and shared memory is a host array.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#define ASARF_HD __host__ __device__
+
+#if defined(__CUDA_ARCH__)
+#define ASARF_INLINE __forceinline__
+#define ASARF_SYNC() __syncthreads()
+#define ASARF_LDG(p) __ldg(p)
+#else
+#define ASARF_INLINE inline
+#define ASARF_SYNC() \
+    do {             \
+    } while (0)
+#define ASARF_LDG(p) (*(p))
+#endif
+
+namespace asarf {
+
+// Integer add into an accumulator shared by many threads.  Integer sums are order
+// independent, so the statistics are bit-reproducible run to run.
+ASARF_HD ASARF_INLINE void atomic_add_u64(unsigned long long* p, unsigned long long v) {
+#if defined(__CUDA_ARCH__)
+    atomicAdd(p, v);
+#else
+    *p += v;
+#endif
+}
+
+ASARF_HD ASARF_INLINE void atomic_add_i64(long long* p, long long v) {
+#if defined(__CUDA_ARCH__)
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+#else
+    *p += v;
+#endif
+}
+
+// IEEE round-to-nearest division and fused multiply-add, written explicitly so the host
+// emulation and the device agree with each other and with nvcc's default contraction.
+ASARF_HD ASARF_INLINE float fdiv_rn(float a, float b) {
+#if defined(__CUDA_ARCH__)
+    return __fdiv_rn(a, b);
+#else
+    return a / b;
+#endif
+}
+
+ASARF_HD ASARF_INLINE float fma_rn(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+    return __fmaf_rn(a, b, c);
+#else
+    return __builtin_fmaf(a, b, c);
+#endif
+}
+
+ASARF_HD ASARF_INLINE float fmul_rn(float a, float b) {
+#if defined(__CUDA_ARCH__)
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+
+ASARF_HD ASARF_INLINE float fadd_rn(float a, float b) {
+#if defined(__CUDA_ARCH__)
+    return __fadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+
+ASARF_HD ASARF_INLINE float fsub_rn(float a, float b) {
+#if defined(__CUDA_ARCH__)
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+
+}  // namespace asarf

@@ -1,0 +1,149 @@
+// Plain-data structures shared by the host planner and the kernels.
+#pragma once
+
+#include <cstdint>
+
+#include "fft.cuh"
+
+namespace asarf {
+
+constexpr int kMaxDcBlocks = 80;   // CalculateDopplerCentroid uses XSize/32-wide blocks (32 or 33 of them)
+constexpr int kRcmcTaps = 16;      // RCMC interpolator length (reference: RCMC_INTERPOLATOR_SIZE 16)
+constexpr int kNumTailVariants = 2;
+
+// Integer accumulators of the raw-statistics pass (zeroed before every run).
+//   mom: filled-sample count, sum I, sum Q, sum I^2, sum Q^2, sum I*Q
+//   lag[b]: over azimuth-adjacent sample pairs (y-1, y) that are both filled, in Doppler
+//           block b: n, sum A, sum B, sum C, sum D, sum AC, sum BD, sum AD, sum BC with
+//           (A, B) = raw (I, Q) of line y-1 and (C, D) = raw (I, Q) of line y.
+struct StatAccum {
+    unsigned long long mom[6];
+    unsigned long long lag[kMaxDcBlocks][9];
+};
+
+// Per-column-independent output of the statistics finalisation, read by later kernels.
+struct FocusState {
+    float dc_i, dc_q, gain, sin_c, cos_c;  // IQ correction as the reference applies it
+    float dc_poly32[3];                    // Doppler centroid polynomial (float, highest power first)
+    double dc_poly[3];
+    double dc_i_d, dc_q_d, iq_gain, phase_error, stddev_i, stddev_q;
+    int nblk;
+    double dc_blk_hz[kMaxDcBlocks];
+    int variant;     // tail variant: 0 when the DC constant term > 0, else 1
+    int first_line;  // first azimuth line kept by the results window
+    int n_lines;     // kept lines
+    unsigned int errors;
+};
+
+enum ErrorBits : unsigned int {
+    kErrRcmcHalo = 1u << 0,      // an RCMC tap fell outside the loaded range halo
+    kErrSrgrIndex = 1u << 1,     // an SRGR index fell outside the slant row
+    kErrStatsEmpty = 1u << 2,    // no filled samples
+    kErrDcBlocks = 1u << 3,      // too many Doppler blocks
+};
+
+// Everything the statistics finalisation needs besides the accumulators.
+struct FinalizeArgs {
+    const StatAccum* acc;
+    FocusState* state;
+    long long n_total;       // CorrectionParams::n_total_samples
+    long long n_pad;         // range-padding samples entering the gain / phase sums
+    int nr;                  // range samples (XSize)
+    int na;                  // azimuth lines (YSize)
+    int rg_stride;           // reference XStride (for Doppler blocks that run into the padding)
+    int dc_step;             // Doppler block width (XSize / 32)
+    int nblk;
+    double prf;
+    // results window inputs (CalcResultsWindow)
+    int lines_before, lines_after, max_aperture;
+    int first_line[kNumTailVariants];
+    int n_lines[kNumTailVariants];
+};
+
+struct RawStatsArgs {
+    const uint8_t* raw;
+    long long line_bytes;
+    int spl;              // I/Q sample pairs per raw record
+    int na, nr;
+    const uint16_t* swst; // nullable
+    int min_swst;
+    int dc_step, nblk;
+    int lines_per_cta;
+    StatAccum* acc;
+};
+
+struct RangeCompressArgs {
+    const uint8_t* raw;
+    long long line_bytes;
+    int spl;
+    int na, nr;
+    const uint16_t* swst;
+    int min_swst;
+    const FocusState* state;
+    FftPlan plan;
+    const float2* mf;     // matched filter in the forward transform's digit-reversed order, / L
+    int nk;
+    float2* out;
+    long long out_pitch;
+};
+
+struct AzStridedArgs {
+    const float2* in;
+    float2* out;
+    long long pitch;
+    int n1, n2;
+    FftPlan plan1;
+    const int* drev1;
+    const float2* twn;    // exp(-2 pi i m / N), N = n1 * n2
+    int nk;
+    int xt;               // columns per block
+    int valid_rows;       // forward: rows at or beyond this are zero
+    const FocusState* state;  // inverse: rows outside the results window are not stored
+    float scale;          // inverse: 1 / N as the reference multiplies
+    int inverse;
+};
+
+struct ColParams {
+    float dc, vr, dc_off, ka, cut_lo, cut_hi;
+    double r0;
+};
+
+struct AzRdArgs {
+    const float2* in;
+    float2* out;
+    long long pitch;
+    int n1, n2, az_pad;
+    FftPlan plan2;
+    const int* drev2;
+    int nk;
+    int xt, hl, hr, wt;
+    int chunk_rows;
+    float prf, lambda, frac;
+    double slant, range_spacing;
+    float vr_poly[3];
+    const FocusState* state;
+    const float* win;     // 16 RCMC window taps
+};
+
+struct TailVariant {
+    int n_lines;
+    int out_az;
+    float ratio;
+    int ng;
+    float grsr[5];
+    const float* rsl;     // nx gains
+};
+
+struct TailArgs {
+    const float2* slc;
+    long long pitch;
+    const FocusState* state;
+    int col0, nx;
+    TailVariant tail[kNumTailVariants];
+    float range_spacing;
+    float ground_spacing;
+    float* out;
+    int out_pitch;
+};
+
+}  // namespace asarf

@@ -1,0 +1,162 @@
+/*
+ * asar-focus B200 — C ABI of the range-Doppler focusing path.
+ *
+ * Plain C: fixed-width integers, doubles, and raw pointers.  Device pointers are CUDA
+ * global-memory addresses on the current device; `stream` is a cudaStream_t (NULL = the
+ * legacy default stream).  Every function returns ASARF_OK (0) or a negative status and
+ * never throws; asarf_last_error() gives the message of the last failure on the calling
+ * thread.  Nothing here allocates inside asarf_focus*(): all device memory is taken at
+ * plan creation, so a focus call can be captured into a CUDA graph.
+ *
+ * Each entry point names the reference interface it replaces (paths relative to the
+ * cgi-estonia-space/asar-focus source tree, v0.3.2).
+ */
+#ifndef ASARF_H_
+#define ASARF_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASARF_OK 0
+#define ASARF_ERR_INVALID (-1)   /* bad argument; reference: std::logic_error / CHECK_BOOL */
+#define ASARF_ERR_CUDA (-2)      /* CUDA runtime error; reference: alus::CudaErrorException */
+#define ASARF_ERR_NOMEM (-3)     /* allocation failed */
+#define ASARF_ERR_NUMERIC (-4)   /* non-convergence (geolocation) / degenerate fit */
+
+/* One orbit state vector (sar/orbit_state_vector.h:24-32); time in microseconds. */
+typedef struct asarf_osv {
+    int64_t time_us;
+    double pos[3];
+    double vel[3];
+} asarf_osv;
+
+/* Scene description: the fields of SARMetadata (sar/sar_metadata.h:57-88) that the
+ * focusing path reads, plus the raw record layout of the ERS byte-I/Q decoder. */
+typedef struct asarf_scene {
+    int32_t range_size;        /* XSize of the decoded image: samples_per_line + 4*(max_swst-min_swst) */
+    int32_t azimuth_size;      /* YSize: number of echo lines */
+    int32_t samples_per_line;  /* I/Q byte pairs per raw record */
+    int32_t raw_line_bytes;    /* byte stride of raw records (even, >= 2*samples_per_line) */
+    int64_t total_raw_samples; /* CorrectionParams::n_total_samples (sar/iq_correction.cuh:22-25) */
+    /* ChirpInfo (sar/sar_metadata.h:34-44) */
+    double range_sampling_rate;
+    double chirp_kr;
+    double pulse_duration;
+    int32_t chirp_samples;     /* round(pulse_duration * fs) (main_flow.cc:391) */
+    int32_t apply_window;      /* range Hamming window on the replica */
+    /* radar / geometry */
+    double prf;
+    double wavelength;
+    double carrier_frequency;
+    double range_spacing;
+    double slant_range_first;
+    double azimuth_spacing;    /* AzimuthMultiLook ratio = 12.5 / azimuth_spacing */
+    double az_bw_frac;         /* processed azimuth bandwidth / PRF */
+    double vr_poly[3];         /* processing velocity polynomial (range pixel), highest power first */
+    int32_t vr_poly_given;     /* 0: estimate it from the orbit (EstimateProcessingVelocity) */
+    double vr_poly_init[3];    /* metadata Vr guess used for aperture lengths (main_flow.cc:465-473) */
+    int32_t n_osv;
+    const asarf_osv* osv;
+    int64_t first_line_time_us;
+    double line_time_interval;
+    double center_point[3];    /* ECEF scene centre, initial guess of every geolocation */
+    int32_t lines_before;      /* lines cached before sensing start (CalcResultsWindow) */
+    int32_t lines_after;       /* lines cached after sensing stop */
+} asarf_scene;
+
+/* Options of the fused plan. */
+typedef struct asarf_options {
+    int32_t rc_fft_len;        /* range FFT length; 0 = auto (any >= range_size gives the same result) */
+    int32_t ref_compat_stats;  /* 1 (default): gain/phase sums include the range padding as the reference does */
+    int32_t iq_padding_ref;    /* range padding the reference would use for those sums; 0 = its own rule */
+} asarf_options;
+
+/* Output geometry of a plan (both tail variants: the Doppler-centroid sign picks one). */
+typedef struct asarf_dims {
+    int32_t nk;                /* range samples after range compression */
+    int32_t rg_pad_ref, az_pad;
+    int32_t rc_fft_len, n1, n2;
+    int32_t slc_cols;          /* nk - 16 */
+    int32_t out_rows[2];       /* multilooked lines, variant 0 (DC > 0) / 1 */
+    int32_t out_cols[2];       /* ground-range samples */
+    int32_t out_rows_max, out_cols_max;
+    int32_t max_aperture;
+    double vr_poly[3];
+    size_t device_bytes;       /* device memory held by the plan */
+} asarf_dims;
+
+/* Per-run results: SARResults (sar/sar_metadata.h:46-55) plus the chosen window. */
+typedef struct asarf_results {
+    double dc_i, dc_q, iq_gain, phase_error, stddev_i, stddev_q;
+    double doppler_centroid_poly[3];
+    double vr_poly[3];
+    int32_t n_dc_blocks;
+    double dc_block_hz[80];
+    int32_t variant, first_line, n_lines, out_rows, out_cols;
+    uint32_t errors;
+} asarf_results;
+
+typedef struct asarf_plan asarf_plan;
+
+const char* asarf_last_error(void);
+const char* asarf_version(void);
+
+void asarf_default_options(asarf_options* opt);
+
+/* Plan one scene shape: sizes, FFT schedules, chirp matched filter, Vr polynomial, SRGR
+ * polynomials, device buffers.  Replaces the setup in main.cc:213-269 (FFT sizes, chirp,
+ * Vr estimation, workspace allocation). */
+int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt, asarf_plan** out);
+void asarf_plan_destroy(asarf_plan* plan);
+int asarf_plan_dims(const asarf_plan* plan, asarf_dims* dims);
+
+/* Focus one scene from device-resident raw bytes to the detected ground-range image
+ * (float [out_rows][out_cols_max], row pitch out_cols_max).  Replaces main.cc:233-327:
+ * ConvertErsImSamplesToComplex + RawDataCorrection + ZeroNaNs + CalculateDopplerCentroid +
+ * RangeCompression + RangeDopplerAlgorithm + SubsetResultsAndReassembleMeta +
+ * AzimuthMultiLook + RangeSpreadingLossCorrection + SlantRangeToGroundRangeInterpolation.
+ * swst may be NULL (all lines start at range sample 0). Asynchronous on `stream`. */
+int asarf_focus(asarf_plan* plan, const uint8_t* d_raw, const uint16_t* d_swst, int32_t min_swst, float* d_out,
+                void* stream);
+
+/* Same from HOST buffers: copies raw bytes (and SWST codes) in, the image out, inside the
+ * call, then synchronises `stream`.  Host buffers may be pageable or pinned. */
+int asarf_focus_host(asarf_plan* plan, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst, float* h_out,
+                     void* stream);
+
+/* Copy the complex subset SLC (IMS tail input) of the last run: complex float
+ * [n_lines][slc_cols] into d_slc (row pitch slc_cols).  Asynchronous. */
+int asarf_plan_slc(asarf_plan* plan, void* d_slc, void* stream);
+
+/* Results of the last run (synchronises `stream`). */
+int asarf_plan_results(asarf_plan* plan, asarf_results* res, void* stream);
+
+/* ---------------------------------------------------------------- host FP64 geometry */
+
+/* InterpolateOrbit (sar/orbit_state_vector.cc:23-48). */
+int asarf_interpolate_orbit(const asarf_osv* osv, int32_t n, int64_t time_us, asarf_osv* out);
+/* RangeDopplerGeoLocate (util/src/geo_tools.cc:27-85). */
+int asarf_geolocate(const double vel[3], const double pos[3], const double init_guess[3], double slant_range,
+                    double out_xyz[3]);
+/* Polyfit (util/src/math_utils.cc:23-44), highest power first, n <= 128, degree <= 4. */
+int asarf_polyfit(const double* x, const double* y, int32_t n, int32_t degree, double* coeffs);
+/* EstimateProcessingVelocity (sar/processing_velocity_estimation.cc:105-148). */
+int asarf_estimate_processing_velocity(const asarf_scene* scene, double vr_poly[3]);
+/* GenerateChirpData (sar/sar_chirp.cc:70-104): padded, windowed, power-normalised replica. */
+int asarf_generate_chirp(double kr, double fs, int32_t n_samples, int32_t apply_window, int32_t padding,
+                         float* out_interleaved);
+/* SRGR polynomial of SlantRangeToGroundRangeInterpolation (sar/srgr.cu:73-121). */
+int asarf_srgr_polynomial(const asarf_scene* scene, double slant_first, int32_t range_size, int32_t azimuth_size,
+                          double line_time_interval, double poly[5], int32_t* ground_samples);
+/* GetOptimalFFTSizes().upper_bound(v) (cuda_util/cufft_plan.cc:147-181, main.cc:217,223). */
+int32_t asarf_fft_size_above(int32_t v);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ASARF_H_ */
