@@ -41,7 +41,7 @@ class FocusPlan:
     takes host arrays and does the copies inside (the end-to-end path)."""
 
     def __init__(self, scene: Scene, rc_fft_len: int = 0, ref_compat_stats: bool = True, lib=None,
-                 lib_path=None):
+                 lib_path=None, dc_poly=None):
         self.lib = lib or load_library(lib_path)
         self.scene = scene
         if scene.vr_poly is None or not scene.osv:
@@ -51,6 +51,9 @@ class FocusPlan:
         self.lib.asarf_default_options(C.byref(opt))
         opt.rc_fft_len = int(rc_fft_len)
         opt.ref_compat_stats = int(bool(ref_compat_stats))
+        if dc_poly is not None:
+            opt.dc_poly_given = 1
+            opt.dc_poly = (C.c_double * 3)(*[float(v) for v in dc_poly])
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_plan_create(C.byref(self._sc), C.byref(opt), C.byref(h)), "plan_create")
         self._h = h
@@ -95,6 +98,11 @@ class FocusPlan:
         r = self.results(stream)
         return out[: r["out_rows"], : r["out_cols"]]
 
+    def focus_host_ptr(self, raw_ptr: int, out_ptr: int, swst_ptr: int = 0, min_swst: int = 0, stream: int = 0):
+        """asarf_focus_host on raw host pointers (e.g. pinned torch tensors); synchronous."""
+        _lib.check(self.lib, self.lib.asarf_focus_host(self._h, raw_ptr, swst_ptr or None, int(min_swst), out_ptr,
+                                                       C.c_void_p(stream)), "focus_host")
+
     def results(self, stream: int = 0) -> dict:
         r = _lib.Results()
         _lib.check(self.lib, self.lib.asarf_plan_results(self._h, C.byref(r), C.c_void_p(stream)), "plan_results")
@@ -104,6 +112,18 @@ class FocusPlan:
             d[f] = list(v) if not isinstance(v, (int, float)) else v
         d["dc_block_hz"] = d["dc_block_hz"][: d["n_dc_blocks"]]
         return d
+
+    def enable_timing(self, runs: int) -> None:
+        """Record events between the kernels of the next ``runs`` focus calls."""
+        _lib.check(self.lib, self.lib.asarf_plan_enable_timing(self._h, int(runs)), "enable_timing")
+
+    def kernel_times(self) -> tuple[dict, int]:
+        """({kernel: total ms over the recorded runs}, runs)."""
+        ms = (C.c_float * 7)()
+        names = (C.c_char_p * 7)()
+        runs = C.c_int32()
+        _lib.check(self.lib, self.lib.asarf_plan_kernel_times(self._h, ms, C.byref(runs), names), "kernel_times")
+        return {names[k].decode(): float(ms[k]) for k in range(7)}, int(runs.value)
 
     def slc_into(self, dst, stream: int = 0):
         """Copy the subset complex image of the last run into ``dst`` (complex64

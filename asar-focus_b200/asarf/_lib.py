@@ -30,7 +30,8 @@ class SceneC(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("rc_fft_len", C.c_int32), ("ref_compat_stats", C.c_int32), ("iq_padding_ref", C.c_int32)]
+    _fields_ = [("rc_fft_len", C.c_int32), ("ref_compat_stats", C.c_int32), ("iq_padding_ref", C.c_int32),
+                ("dc_poly_given", C.c_int32), ("dc_poly", C.c_double * 3)]
 
 
 class Dims(C.Structure):
@@ -46,6 +47,7 @@ class Results(C.Structure):
     _fields_ = [
         ("dc_i", C.c_double), ("dc_q", C.c_double), ("iq_gain", C.c_double), ("phase_error", C.c_double),
         ("stddev_i", C.c_double), ("stddev_q", C.c_double), ("doppler_centroid_poly", C.c_double * 3),
+        ("doppler_centroid_estimate", C.c_double * 3),
         ("vr_poly", C.c_double * 3), ("n_dc_blocks", C.c_int32), ("dc_block_hz", C.c_double * 80),
         ("variant", C.c_int32), ("first_line", C.c_int32), ("n_lines", C.c_int32), ("out_rows", C.c_int32),
         ("out_cols", C.c_int32), ("errors", C.c_uint32),
@@ -67,6 +69,9 @@ _SIGS = {
     "asarf_focus_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "asarf_plan_slc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "asarf_plan_results": (C.c_int, [C.c_void_p, C.POINTER(Results), C.c_void_p]),
+    "asarf_plan_enable_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "asarf_plan_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_char_p)]),
     "asarf_interpolate_orbit": (C.c_int, [C.POINTER(Osv), C.c_int32, C.c_int64, C.POINTER(Osv)]),
     "asarf_geolocate": (C.c_int, [C.POINTER(C.c_double * 3)] * 3 + [C.c_double, C.POINTER(C.c_double * 3)]),
     "asarf_polyfit": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32, C.c_int32,

@@ -283,8 +283,15 @@ def tiny(**kw) -> Scene:
     return Scene(**base)
 
 
+def ers_mid(**kw) -> Scene:
+    """5616 x 8192 cut of the ERS scene: profiling case (complex images 324 MB, above L2)."""
+    base = dict(name="ers_mid", azimuth_size=8192, grid=(10, 6))
+    base.update(kw)
+    return ers_full(**base)
+
+
 WORKLOADS = {"ers_small": ers_small, "ers_full": ers_full, "asar_im": asar_im, "asar_strip": asar_strip,
-             "tiny": tiny}
+             "tiny": tiny, "ers_mid": ers_mid}
 
 
 def with_sizes(sc: Scene, **kw) -> Scene:

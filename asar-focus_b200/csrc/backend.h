@@ -29,6 +29,10 @@ int mem_d2d(void* dst, const void* src, size_t n, void* stream);
 int mem_d2d_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t rows, void* stream);
 int mem_zero(void* dst, size_t n, void* stream);
 int stream_sync(void* stream);
+void* event_create();
+void event_destroy(void* e);
+int event_record(void* e, void* stream);
+int event_elapsed(void* a, void* b, float* ms);
 size_t smem_optin_limit();
 const char* backend_name();
 

@@ -276,6 +276,11 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
     st.nblk = nblk;
     double poly[3] = {0.0, 0.0, 0.0};
     polyfit_qr<kMaxDcBlocks, 3>(xs, ys, nblk, 2, poly);
+    st.dc_est[0] = poly[0];
+    st.dc_est[1] = poly[1];
+    st.dc_est[2] = poly[2];
+    if (a.dc_given)
+        for (int k = 0; k < 3; ++k) poly[k] = a.dc_in[k];
     for (int k = 0; k < 3; ++k) {
         st.dc_poly[k] = poly[k];
         st.dc_poly32[k] = static_cast<float>(poly[k]);

@@ -79,6 +79,13 @@ int mem_zero(void* dst, size_t n, void*) {
     return ASARF_OK;
 }
 int stream_sync(void*) { return ASARF_OK; }
+void* event_create() { return std::calloc(1, 8); }
+void event_destroy(void* e) { std::free(e); }
+int event_record(void*, void*) { return ASARF_OK; }
+int event_elapsed(void*, void*, float* ms) {
+    *ms = 0.0f;
+    return ASARF_OK;
+}
 size_t smem_optin_limit() { return 227 * 1024; }
 const char* backend_name() { return "host-emulation"; }
 

@@ -380,6 +380,9 @@ struct asarf_plan {
     LaunchShape sh_rc{}, sh_st{}, sh_rd{}, sh_tail{};
     int tiles1 = 0, tiles2 = 0;
     int out_rows_max = 0, out_cols_max = 0;
+    // optional per-kernel timing (events recorded between the launches of each run)
+    std::vector<void*> events;
+    int timing_slots = 0, timing_used = 0;
 
     template <class T>
     T* alloc(size_t count) {
@@ -391,6 +394,7 @@ struct asarf_plan {
         return static_cast<T*>(p);
     }
     ~asarf_plan() {
+        for (void* e : events) event_destroy(e);
         for (void* p : allocs) mem_free(p);
     }
 };
@@ -409,6 +413,8 @@ void asarf_default_options(asarf_options* opt) {
     opt->rc_fft_len = 0;
     opt->ref_compat_stats = 1;
     opt->iq_padding_ref = 0;
+    opt->dc_poly_given = 0;
+    opt->dc_poly[0] = opt->dc_poly[1] = opt->dc_poly[2] = 0.0;
 }
 
 int32_t asarf_fft_size_above(int32_t v) { return fft_size_above(v); }
@@ -698,6 +704,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     fin.lines_before = s.lines_before;
     fin.lines_after = s.lines_after;
     fin.max_aperture = max_ap;
+    fin.dc_given = opt.dc_poly_given ? 1 : 0;
+    for (int k = 0; k < 3; ++k) fin.dc_in[k] = opt.dc_poly[k];
     for (int v = 0; v < 2; ++v) {
         fin.first_line[v] = first_line[v];
         fin.n_lines[v] = n_lines[v];
@@ -824,35 +832,94 @@ int asarf_plan_dims(const asarf_plan* plan, asarf_dims* dims) {
     return ASARF_OK;
 }
 
+static constexpr int kKernelsPerRun = 7;
+static const char* const kKernelNames[kKernelsPerRun] = {"raw_stats", "finalize", "range_compress", "az_strided_fwd",
+                                                          "az_rd", "az_strided_inv", "tail"};
+
 int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int32_t min_swst, float* d_out,
                 void* stream) {
     if (!p || !d_raw || !d_out) return set_error(ASARF_ERR_INVALID, "focus: null argument");
     if (reinterpret_cast<uintptr_t>(d_raw) & 1) return set_error(ASARF_ERR_INVALID, "raw buffer must be 2-byte aligned");
+    void** ev = nullptr;
+    if (p->timing_used < p->timing_slots) {
+        ev = &p->events[static_cast<size_t>(p->timing_used) * (kKernelsPerRun + 1)];
+        ++p->timing_used;
+    }
+    int k = 0;
+    auto mark = [&]() {
+        if (ev) event_record(ev[k], stream);
+        ++k;
+    };
     int rc = mem_zero(p->acc, sizeof(StatAccum), stream);
     if (rc) return rc;
     RawStatsArgs st = p->a_stats;
     st.raw = d_raw;
     st.swst = d_swst;
     st.min_swst = min_swst;
+    mark();
     rc = backend_raw_stats(st, p->stats_gx, p->stats_gy, 256, p->stats_cols, stream);
     if (rc) return rc;
+    mark();
     rc = backend_finalize(p->a_fin, stream);
     if (rc) return rc;
     RangeCompressArgs r = p->a_rc;
     r.raw = d_raw;
     r.swst = d_swst;
     r.min_swst = min_swst;
+    mark();
     rc = backend_range_compress(r, p->na, p->sh_rc, stream);
     if (rc) return rc;
+    mark();
     rc = backend_az_strided(p->a_fwd, p->tiles1, p->n2, p->sh_st, stream);
     if (rc) return rc;
+    mark();
     rc = backend_az_rd(p->a_rd, p->tiles2, p->n1, p->sh_rd, &p->state->errors, stream);
     if (rc) return rc;
+    mark();
     rc = backend_az_strided(p->a_inv, p->tiles1, p->n2, p->sh_st, stream);
     if (rc) return rc;
     TailArgs t = p->a_tail;
     t.out = d_out;
-    return backend_tail(t, p->out_rows_max, p->sh_tail, &p->state->errors, stream);
+    mark();
+    rc = backend_tail(t, p->out_rows_max, p->sh_tail, &p->state->errors, stream);
+    if (rc) return rc;
+    mark();
+    return ASARF_OK;
+}
+
+int asarf_plan_enable_timing(asarf_plan* p, int32_t runs) {
+    if (!p || runs < 0) return set_error(ASARF_ERR_INVALID, "enable_timing: bad arguments");
+    for (void* e : p->events) event_destroy(e);
+    p->events.clear();
+    p->timing_slots = 0;
+    p->timing_used = 0;
+    for (int i = 0; i < runs * (kKernelsPerRun + 1); ++i) {
+        void* e = event_create();
+        if (!e) return set_error(ASARF_ERR_CUDA, "event creation failed");
+        p->events.push_back(e);
+    }
+    p->timing_slots = runs;
+    return ASARF_OK;
+}
+
+int asarf_plan_kernel_times(asarf_plan* p, float* total_ms, int32_t* runs, const char** names) {
+    if (!p || !total_ms || !runs) return set_error(ASARF_ERR_INVALID, "kernel_times: null argument");
+    for (int k = 0; k < kKernelsPerRun; ++k) {
+        total_ms[k] = 0.0f;
+        if (names) names[k] = kKernelNames[k];
+    }
+    for (int r = 0; r < p->timing_used; ++r) {
+        void** ev = &p->events[static_cast<size_t>(r) * (kKernelsPerRun + 1)];
+        for (int k = 0; k < kKernelsPerRun; ++k) {
+            float ms = 0.0f;
+            int rc = event_elapsed(ev[k], ev[k + 1], &ms);
+            if (rc) return rc;
+            total_ms[k] += ms;
+        }
+    }
+    *runs = p->timing_used;
+    p->timing_used = 0;
+    return ASARF_OK;
 }
 
 int asarf_focus_host(asarf_plan* p, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst, float* h_out,
@@ -887,6 +954,7 @@ int asarf_plan_results(asarf_plan* p, asarf_results* res, void* stream) {
     res->stddev_q = st.stddev_q;
     for (int k = 0; k < 3; ++k) {
         res->doppler_centroid_poly[k] = st.dc_poly[k];
+        res->doppler_centroid_estimate[k] = st.dc_est[k];
         res->vr_poly[k] = p->vr_poly[k];
     }
     res->n_dc_blocks = st.nblk;

@@ -137,6 +137,26 @@ int mem_zero(void* dst, size_t n, void* stream) {
 }
 int stream_sync(void* stream) { return cuda_rc(cudaStreamSynchronize(S(stream)), "stream sync"); }
 
+void* event_create() {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+void event_destroy(void* e) {
+    if (e) cudaEventDestroy(static_cast<cudaEvent_t>(e));
+}
+int event_record(void* e, void* stream) {
+    return cuda_rc(cudaEventRecord(static_cast<cudaEvent_t>(e), S(stream)), "event record");
+}
+int event_elapsed(void* a, void* b, float* ms) {
+    cudaError_t e = cudaEventSynchronize(static_cast<cudaEvent_t>(b));
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, static_cast<cudaEvent_t>(a), static_cast<cudaEvent_t>(b));
+    return cuda_rc(e, "event elapsed");
+}
+
 size_t smem_optin_limit() {
     int dev = 0, v = 0;
     cudaGetDevice(&dev);

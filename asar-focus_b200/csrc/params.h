@@ -25,7 +25,8 @@ struct StatAccum {
 struct FocusState {
     float dc_i, dc_q, gain, sin_c, cos_c;  // IQ correction as the reference applies it
     float dc_poly32[3];                    // Doppler centroid polynomial (float, highest power first)
-    double dc_poly[3];
+    double dc_poly[3];                     // polynomial in use (estimate or the caller's)
+    double dc_est[3];                      // ACCC estimate
     double dc_i_d, dc_q_d, iq_gain, phase_error, stddev_i, stddev_q;
     int nblk;
     double dc_blk_hz[kMaxDcBlocks];
@@ -56,6 +57,8 @@ struct FinalizeArgs {
     double prf;
     // results window inputs (CalcResultsWindow)
     int lines_before, lines_after, max_aperture;
+    int dc_given;            // use dc_in instead of the estimate
+    double dc_in[3];
     int first_line[kNumTailVariants];
     int n_lines[kNumTailVariants];
 };

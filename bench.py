@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Benchmark of the range-Doppler focusing path on B200.
+
+Metric: raw Msamples/s focused = (range samples x azimuth lines of every scene) / time.
+One step = one full focus of one ERS-like 5616 x 28000 5-bit scene (the BASELINE's
+single-GPU configuration): raw I/Q bytes resident in HBM -> IQ statistics + Doppler
+centroid -> range compression -> azimuth FFT / RCMC / matched filter / IFFT -> results
+window -> 5-look multilook + range spreading loss -> slant-to-ground resampling.
+The scene is synthetic (seeded point-target grid on clutter), generated on the device.
+
+Multi-GPU: one process per GPU (torchrun), each rank focuses its own scene (independent
+units, no data-path collective: weak scaling); timing is the max over ranks.
+
+--impl reference runs the reference's own CUDA build (oracle/_ref/libasar_ref.so, the
+asar-focus sar/ + cuda_util/ sources compiled for sm_100a with cuFFT) on the same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "asar-focus_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "raw Msamples/s focused on 1 B200 (ERS-like 5616x28000, plain FP32)"
+UNIT = "Msamples/s"
+HBM_FALLBACK = 6650.0
+KERNELS = ["raw_stats", "finalize", "range_compress", "az_strided_fwd", "az_rd", "az_strided_inv", "tail"]
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend=backend, timeout=timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def _max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_scene(workload: str, seed: int):
+    from asarf import scene as S
+    return S.WORKLOADS[workload](seed=seed)
+
+
+def algorithmic_bytes(sc, dims: dict, res: dict) -> dict:
+    """Minimal HBM bytes each kernel must move (inputs read once, outputs written once,
+    no halo, no padding rows), per launch."""
+    na, spl = sc.azimuth_size, sc.samples_per_line
+    nk, az = dims["nk"], dims["az_pad"]
+    nx = dims["slc_cols"]
+    raw = na * 2 * spl
+    nl = res["n_lines"]
+    out = res["out_rows"] * res["out_cols"] * 4
+    return {"raw_stats": raw, "finalize": 0, "range_compress": raw + na * nk * 8,
+            "az_strided_fwd": na * nk * 8 + az * nk * 8, "az_rd": 2 * az * nk * 8,
+            "az_strided_inv": az * nk * 8 + nl * nk * 8, "tail": nl * nx * 8 + out}
+
+
+def pipeline_bytes(sc, dims: dict, res: dict) -> float:
+    """Algorithmic bytes of the whole scene: raw read twice, two complex round trips,
+    multilooked float round trip, ground-range output write (unpadded sizes)."""
+    na, nr = sc.azimuth_size, sc.range_size
+    nk = dims["nk"]
+    L = 5.0
+    ng = res["out_cols"]
+    return na * 2 * nr * 2 + 32 * nk * na + 8 * nk * na / L + 4 * ng * na / L
+
+
+def _traffic_from_profiles(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if one exists."""
+    for f in sorted((ROOT / "profiles").glob(f"*{kernel}*{workload}*.txt")):
+        for line in f.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    pass
+    return None
+
+
+def cpu_baseline(sc_full, raw_full) -> dict:
+    """The FP64 CPU oracle on a bounded sample: the first 4096 lines of the same scene."""
+    import numpy as np
+    from dataclasses import replace
+    from oracle import rda
+    lines = 4096
+    sc = replace(sc_full, azimuth_size=lines)
+    sc.vr_poly = sc_full.vr_poly
+    raw = np.ascontiguousarray(raw_full[:lines])
+    t0 = time.perf_counter()
+    rda.focus(raw, sc.to_dict())
+    dt = time.perf_counter() - t0
+    n = sc.range_size * lines
+    return {"value": round(n / dt / 1e6, 3), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"first {lines} lines of the {sc_full.range_size}x{sc_full.azimuth_size} scene "
+                      f"({n / 1e6:.1f} Msamples) through the numpy FP64 oracle (scipy.fft workers=all cores), "
+                      f"{dt:.1f} s"}
+
+
+def run_ours(args, rank: int, world: int, local: int) -> None:
+    import numpy as np
+    import torch
+    import asarf
+    from asarf import sim
+
+    lib = asarf.load_library()
+    sc = make_scene(args.workload, 1001 + rank)
+    sc.prepare(lib)
+    plan = asarf.FocusPlan(sc, lib=lib)
+    raw_np, _ = sim.simulate(sc, device="cuda")
+    raw_d = torch.from_numpy(raw_np).cuda()
+    out_d = torch.empty(plan.out_shape, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    st = stream.cuda_stream
+    for _ in range(args.warmup):
+        plan.focus(raw_d, out_d, stream=st)
+    torch.cuda.synchronize()
+    res = plan.results()
+    if res["errors"]:
+        raise RuntimeError(f"focus reported error flags {res['errors']:#x}")
+    _barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.25)
+    plan.enable_timing(args.steps)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    _barrier(world)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.focus(raw_d, out_d, stream=st)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    clocks = sampler.stop()
+    ms_step = e0.elapsed_time(e1) / args.steps
+    ktimes, kruns = plan.kernel_times()
+    ms_max = _max_over_ranks(ms_step, world)
+    samples = sc.range_size * sc.azimuth_size
+    value = samples * world / ms_max / 1e3
+
+    # end to end through the public host API: pinned raw in, detected image out, every step
+    raw_h = torch.from_numpy(raw_np).pin_memory()
+    out_h = torch.empty(plan.out_shape, dtype=torch.float32).pin_memory()
+    plan.focus_host_ptr(raw_h.data_ptr(), out_h.data_ptr(), stream=st)
+    e2e_steps = max(3, min(args.steps, 20))
+    torch.cuda.synchronize()
+    _barrier(world)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(e2e_steps):
+        plan.focus_host_ptr(raw_h.data_ptr(), out_h.data_ptr(), stream=st)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = _max_over_ranks(t0.elapsed_time(t1) / e2e_steps, world)
+    e2e_value = samples * world / e2e_ms / 1e3
+
+    res = plan.results()
+    dims = plan.dims
+    alg = algorithmic_bytes(sc, dims, res)
+    per_launch = {k: ktimes[k] / max(kruns, 1) for k in KERNELS}
+    dom = max(per_launch, key=per_launch.get)
+    peaks = _peaks()
+    peak = float(peaks.get("hbm_gbs", HBM_FALLBACK))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = alg[dom] / (per_launch[dom] * 1e-3) / 1e9
+    traffic = _traffic_from_profiles(dom, args.workload)
+    pipe = pipeline_bytes(sc, dims, res)
+
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32 (complex64 data, FP64 geometry)", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: ERS-like {sc.range_size} range x {sc.azimuth_size} azimuth, "
+                               f"{sc.bits}-bit I/Q, 20x20 point grid, DC 250..350 Hz, Vr from 5 orbit vectors",
+                   "range_samples": sc.range_size, "azimuth_lines": sc.azimuth_size, "scenes_per_step": world,
+                   "l2": "inputs larger than L2 (raw 314 MB, complex images 1.1 GB each)",
+                   "parallelism": f"replicas x{world} (independent scenes)",
+                   "az_pad": dims["az_pad"], "rc_fft_len": dims["rc_fft_len"]},
+        "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
+                "h2d_bytes_per_step": int(raw_np.nbytes), "d2h_bytes_per_step": int(out_h.numel() * 4),
+                "ms_per_step": round(e2e_ms, 4), "api": "asarf_focus_host (pinned host buffers)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
+                     "algorithmic_bytes_per_launch": int(alg[dom]), "ms_per_launch": round(per_launch[dom], 4)},
+        "pipeline_roofline": {"algorithmic_bytes": int(pipe), "achieved": round(pipe / (ms_max * 1e-3) / 1e9, 1),
+                              "frac": round(pipe / (ms_max * 1e-3) / 1e9 / peak, 4), "unit": "GB/s"},
+        "kernel_ms_per_step": {k: round(v, 4) for k, v in per_launch.items()},
+        "gpu_launches": 7 * args.steps,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc, raw_np)
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+    import asarf
+    from asarf import sim
+    from oracle import ref_lib
+
+    if not ref_lib.available():
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build missing ({ref_lib.REF_LIB})"}))
+        return
+    lib = asarf.load_library()
+    sc = make_scene(args.workload, 1001)
+    sc.prepare(lib)
+    raw_np, _ = sim.simulate(sc, device="cuda")
+    raw_d = torch.from_numpy(raw_np).cuda()
+    scc, keep = sc.to_c()
+    cap = sc.azimuth_size * sc.range_size
+    for _ in range(args.warmup):
+        ref_lib.ref_focus(scc, sc.vr_poly, raw_np, out_capacity=cap, d_raw_ptr=raw_d.data_ptr())
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.25)
+    dev_ms, wall = [], []
+    for _ in range(args.steps):
+        _, r, _ = ref_lib.ref_focus(scc, sc.vr_poly, raw_np, out_capacity=cap, d_raw_ptr=raw_d.data_ptr())
+        dev_ms.append(r["ms_total"])
+        wall.append(r["ms_wall"])
+    e2e = []
+    for _ in range(max(3, min(args.steps, 10))):
+        _, r, _ = ref_lib.ref_focus(scc, sc.vr_poly, raw_np, out_capacity=cap)
+        e2e.append(r["ms_wall"])
+    clocks = sampler.stop()
+    samples = sc.range_size * sc.azimuth_size
+    ms = statistics.mean(dev_ms)
+    value = samples / ms / 1e3
+    e2e_ms = statistics.mean(e2e)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (cuFFT)", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: ERS-like {sc.range_size} range x {sc.azimuth_size} azimuth "
+                               f"(same seeded scene as the optimised arm)",
+                   "range_samples": sc.range_size, "azimuth_lines": sc.azimuth_size,
+                   "l2": "inputs larger than L2", "parallelism": "single GPU"},
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "the reference's own CUDA build (asar-focus sar/ + cuda_util/, cuFFT) on this "
+                                   "B200, driven by one host thread; the reference has no CPU implementation"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "host_api_value": round(samples / e2e_ms / 1e3, 1),
+                "host_api_note": "wall clock through ConvertErsImSamplesToComplex (host raw) to host output"},
+        "device_ms_steps": [round(v, 2) for v in dev_ms],
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="ers_full")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    rank, world, local = _dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        import torch.distributed as dist
+        if dist.is_initialized():
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -73,6 +73,8 @@ typedef struct asarf_options {
     int32_t rc_fft_len;        /* range FFT length; 0 = auto (any >= range_size gives the same result) */
     int32_t ref_compat_stats;  /* 1 (default): gain/phase sums include the range padding as the reference does */
     int32_t iq_padding_ref;    /* range padding the reference would use for those sums; 0 = its own rule */
+    int32_t dc_poly_given;     /* 1: use dc_poly instead of the ACCC estimate (the estimate is still reported) */
+    double dc_poly[3];         /* Doppler centroid polynomial (range pixel), highest power first */
 } asarf_options;
 
 /* Output geometry of a plan (both tail variants: the Doppler-centroid sign picks one). */
@@ -92,7 +94,8 @@ typedef struct asarf_dims {
 /* Per-run results: SARResults (sar/sar_metadata.h:46-55) plus the chosen window. */
 typedef struct asarf_results {
     double dc_i, dc_q, iq_gain, phase_error, stddev_i, stddev_q;
-    double doppler_centroid_poly[3];
+    double doppler_centroid_poly[3];     /* polynomial used (estimate unless overridden) */
+    double doppler_centroid_estimate[3]; /* ACCC estimate (CalculateDopplerCentroid) */
     double vr_poly[3];
     int32_t n_dc_blocks;
     double dc_block_hz[80];
@@ -131,6 +134,15 @@ int asarf_focus_host(asarf_plan* plan, const uint8_t* h_raw, const uint16_t* h_s
 /* Copy the complex subset SLC (IMS tail input) of the last run: complex float
  * [n_lines][slc_cols] into d_slc (row pitch slc_cols).  Asynchronous. */
 int asarf_plan_slc(asarf_plan* plan, void* d_slc, void* stream);
+
+/* Per-kernel timing: record CUDA events between the kernel launches of the next `runs`
+ * asarf_focus calls (0 disables).  No counterpart in the reference (it has wall-clock
+ * TimeStart/TimeStop logging only, main.cc:63-69). */
+int asarf_plan_enable_timing(asarf_plan* plan, int32_t runs);
+/* Sum of each kernel's event-timed duration over the recorded runs (7 kernels: raw_stats,
+ * finalize, range_compress, az_strided_fwd, az_rd, az_strided_inv, tail); synchronises on
+ * the events, then clears them.  `names` (optional) receives 7 static strings. */
+int asarf_plan_kernel_times(asarf_plan* plan, float* total_ms, int32_t* runs, const char** names);
 
 /* Results of the last run (synchronises `stream`). */
 int asarf_plan_results(asarf_plan* plan, asarf_results* res, void* stream);

@@ -28,36 +28,6 @@ def _workers() -> int:
 
 # --------------------------------------------------------------------------- float32 helpers
 
-def fmaf_vec(a, b, c) -> np.ndarray:
-    """Vectorised exact float32 fma: a*b exact in binary64, TwoSum residual resolves ties."""
-    a = np.asarray(a, dtype=np.float32).astype(np.float64)
-    b = np.asarray(b, dtype=np.float32).astype(np.float64)
-    c = np.asarray(c, dtype=np.float32).astype(np.float64)
-    p = a * b
-    s = p + c
-    bb = s - p
-    err = (p - (s - bb)) + (c - bb)
-    r = s.astype(np.float32)
-    # s exactly halfway between two float32 values: the residual decides
-    rd = r.astype(np.float64)
-    up = np.nextafter(r, np.float32(np.inf))
-    dn = np.nextafter(r, np.float32(-np.inf))
-    mid_up = (rd + up.astype(np.float64)) / 2
-    mid_dn = (rd + dn.astype(np.float64)) / 2
-    fix_up = (s == mid_up) & (err > 0)
-    fix_dn = (s == mid_dn) & (err < 0)
-    # r came from ties-to-even on s; if s is a midpoint the residual picks the side
-    r = np.where((s == mid_up) & (err < 0), r, r)
-    r = np.where(fix_up, up, r)
-    r = np.where(fix_dn, dn, r)
-    # when s == mid_up and ties-to-even rounded s up to 'up' already, r holds 'up'; err<0 must give r_lower
-    r_lower_needed = (s.astype(np.float32).astype(np.float64) > s) & (err < 0)
-    r = np.where(r_lower_needed, np.nextafter(s.astype(np.float32), np.float32(-np.inf)), r)
-    r_upper_needed = (s.astype(np.float32).astype(np.float64) < s) & (err > 0)
-    r = np.where(r_upper_needed, np.nextafter(s.astype(np.float32), np.float32(np.inf)), r)
-    return r.astype(np.float32)
-
-
 def _fix_midpoints(s, err):
     """Round binary64 s (+ residual err) to float32 correctly."""
     r = s.astype(np.float32)
@@ -238,15 +208,23 @@ def generate_chirp(kr: float, fs: float, n_samples: int, apply_window: bool, pad
     c = (np.cos(ph).astype(np.float32) + 1j * np.sin(ph).astype(np.float32)).astype(np.complex64)
     if apply_window:
         m = (0.54 - 0.46 * np.cos(2 * np.pi * i / n_samples)).astype(np.float32)
-        c = (c * m).astype(np.complex64)
+        cr = c.real * m
+        ci = c.imag * m
+        c = np.empty_like(c)
+        c.real = cr
+        c.imag = ci
     out = np.zeros(padding, dtype=np.complex64)
     out[:n_samples] = c
     if apply_window:
         scale = float((np.abs(out.astype(np.complex128)) ** 2).sum())
     else:
         scale = float(n_samples)
-    out = (out / F32(math.sqrt(scale))).astype(np.complex64)
-    return out
+    d = F32(math.sqrt(scale))
+    # complex<float> /= float divides each component (a complex division would round differently)
+    res = np.empty_like(out)
+    res.real = out.real / d
+    res.imag = out.imag / d
+    return res
 
 
 def range_compression(img: np.ndarray, y_size: int, x_size: int, chirp: np.ndarray, chirp_samples: int) -> int:

@@ -106,6 +106,15 @@ GeoPos3D RangeDopplerGeoLocate(Velocity3D v, GeoPos3D p, GeoPos3D g, double slan
     throw std::runtime_error("Failed to converge for RangeDopplerGeoLocate");
 }
 
+// The reference's ERS decode kernel (envisat_format/src/envisat_format_kernels.cu:116-134),
+// launched here directly on device-resident raw bytes with the grid its host wrapper uses
+// (the wrapper itself always copies from host memory).
+namespace alus::asar::envformat {
+__global__ void ConvertErsImSamplesToComplexKernel(const uint8_t* samples, int samples_range_size_bytes, int packets,
+                                                   const uint16_t* swst_codes, uint16_t min_swst,
+                                                   cufftComplex* target_buf, int target_range_width);
+}
+
 // ---------------------------------------------------------------- harness entry point
 
 extern "C" {
@@ -124,9 +133,12 @@ typedef struct ref_outputs {
 // Runs the reference chain; optional host dumps (NULL to skip):
 //   corrected [na][nr] complex (after RawDataCorrection + ZeroNaNs), rc [na][nk] complex,
 //   slc [n_lines][nk-16] complex, ml [out_rows][nk-16] float (after RSL).
+// d_raw (optional): device copy of the raw bytes; when given the timed region starts from
+// device-resident input (decode kernel launched directly), otherwise from host memory
+// through the reference's own ConvertErsImSamplesToComplex (which copies internally).
 int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_raw, const uint16_t* h_swst,
               float* h_out, int64_t out_capacity, ref_outputs* o, float* h_corrected, float* h_rc, float* h_slc,
-              float* h_ml) {
+              float* h_ml, const uint8_t* d_raw) {
     std::memset(o, 0, sizeof(*o));
     try {
         auto wall0 = std::chrono::steady_clock::now();
@@ -175,13 +187,26 @@ int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_ra
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventCreate(&e2);
+        uint16_t* d_swst = nullptr;
+        if (d_raw) {
+            CHECK_CUDA_ERR(cudaMalloc(&d_swst, sizeof(uint16_t) * na));
+            CHECK_CUDA_ERR(cudaMemcpy(d_swst, swst.data(), sizeof(uint16_t) * na, cudaMemcpyHostToDevice));
+        }
         cudaEventRecord(e0);
         // ConvertRawSampleSetsToComplex (main_flow.cc:530-583), ERS path
         cufftComplex* d_parsed = nullptr;
         CHECK_CUDA_ERR(cudaMalloc(&d_parsed, sizeof(cufftComplex) * static_cast<size_t>(nr) * na));
         alus::cuda::algorithm::Fill(d_parsed, static_cast<size_t>(nr) * na, cufftComplex{NAN, NAN});
-        alus::asar::envformat::ConvertErsImSamplesToComplex(h_raw, s->samples_per_line, na, swst.data(), min_swst,
-                                                           d_parsed, nr);
+        if (d_raw) {
+            const int x_size = 11232;  // ers::highrate::MEASUREMENT_DATA_SIZE_BYTES, as the wrapper sizes its grid
+            dim3 block(16, 16), grid((x_size + 15) / 16, (na + 15) / 16);
+            alus::asar::envformat::ConvertErsImSamplesToComplexKernel<<<grid, block>>>(
+                d_raw, 2 * s->samples_per_line, na, d_swst, min_swst, d_parsed, nr);
+            CHECK_CUDA_ERR(cudaGetLastError());
+        } else {
+            alus::asar::envformat::ConvertErsImSamplesToComplex(h_raw, s->samples_per_line, na, swst.data(),
+                                                               min_swst, d_parsed, nr);
+        }
         cudaEventRecord(e1);
         // main.cc:213-245
         const auto fft_sizes = GetOptimalFFTSizes();
@@ -280,6 +305,7 @@ int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_ra
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaEventDestroy(e2);
+        if (d_swst) cudaFree(d_swst);
         if (h_out && n_out > out_capacity) {
             std::snprintf(o->error, sizeof(o->error), "output needs %lld floats", static_cast<long long>(n_out));
             return -1;

@@ -1,0 +1,77 @@
+"""ctypes binding of the reference build (oracle/_ref/libasar_ref.so, made by oracle/ref_build).
+
+TEST INFRASTRUCTURE ONLY: the reference's own CUDA focusing code, run on the GPU to pin
+the CPU oracle and to time the reference arm of the benchmark.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+REF_LIB = Path(__file__).resolve().parent / "_ref" / "libasar_ref.so"
+
+
+class RefOutputs(C.Structure):
+    _fields_ = [
+        ("dc_i", C.c_double), ("dc_q", C.c_double), ("iq_gain", C.c_double), ("phase_error", C.c_double),
+        ("stddev_i", C.c_double), ("stddev_q", C.c_double), ("dc_poly", C.c_double * 3),
+        ("grsr_poly", C.c_double * 5), ("first_line", C.c_int32), ("n_lines", C.c_int32),
+        ("slc_cols", C.c_int32), ("out_rows", C.c_int32), ("out_cols", C.c_int32), ("max_aperture", C.c_int32),
+        ("ms_total", C.c_double), ("ms_after_decode", C.c_double), ("ms_wall", C.c_double),
+        ("error", C.c_char * 256),
+    ]
+
+
+_lib = None
+
+
+def available() -> bool:
+    return REF_LIB.exists()
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"reference build missing: {REF_LIB} (make -C oracle/ref_build)")
+        _lib = C.CDLL(str(REF_LIB))
+        f = _lib.ref_focus
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, C.POINTER(C.c_double * 3), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                      C.POINTER(RefOutputs), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    return _lib
+
+
+def ref_focus(scene_c, vr_poly, raw: np.ndarray, swst=None, dumps: bool = False, out_capacity: int | None = None,
+              d_raw_ptr: int = 0):
+    """Run the reference chain on host raw bytes.  Returns (detected float32 [rows, cols],
+    outputs dict, dumps dict)."""
+    lib = load()
+    raw = np.ascontiguousarray(raw, dtype=np.uint8)
+    na, nr = scene_c.azimuth_size, scene_c.range_size
+    nk = nr - scene_c.chirp_samples
+    cap = out_capacity or (na * nr)
+    out = np.empty(cap, dtype=np.float32)
+    d = {}
+    ptrs = [None, None, None, None]
+    if dumps:
+        d["corrected"] = np.empty((na, nr), dtype=np.complex64)
+        d["rc"] = np.empty((na, nk), dtype=np.complex64)
+        d["slc"] = np.empty(na * (nk - 16), dtype=np.complex64)
+        d["ml"] = np.empty(na * (nk - 16), dtype=np.float32)
+        ptrs = [d["corrected"].ctypes.data, d["rc"].ctypes.data, d["slc"].ctypes.data, d["ml"].ctypes.data]
+    sw = None if swst is None else np.ascontiguousarray(swst, dtype=np.uint16)
+    o = RefOutputs()
+    vr = (C.c_double * 3)(*vr_poly)
+    rc = lib.ref_focus(C.addressof(scene_c), vr, raw.ctypes.data, None if sw is None else sw.ctypes.data,
+                       out.ctypes.data, cap, C.byref(o), *ptrs, d_raw_ptr or None)
+    if rc != 0:
+        raise RuntimeError(f"reference chain failed ({rc}): {o.error.decode(errors='replace')}")
+    res = {f: (list(getattr(o, f)) if f in ("dc_poly", "grsr_poly") else getattr(o, f)) for f, _ in o._fields_}
+    det = out[: o.out_rows * o.out_cols].reshape(o.out_rows, o.out_cols)
+    if dumps:
+        d["slc"] = d["slc"][: o.n_lines * o.slc_cols].reshape(o.n_lines, o.slc_cols)
+        d["ml"] = d["ml"][: o.out_rows * o.slc_cols].reshape(o.out_rows, o.slc_cols)
+    return det, res, d

@@ -1,0 +1,78 @@
+"""The exact kernel bodies (host-emulation build) against the CPU oracle, on CPU.
+
+Same code as the sm_100a kernels (bodies.cuh), run single-threaded; a kernel logic error
+shows up here before any GPU time is spent.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import asarf
+from asarf import scene as S
+from conftest import oracle_focus, rel_rmse, scene_and_raw
+
+TOL_DETECTED = 1e-5  # relative RMSE of the detected intensity (float32 FFT vs FP64 oracle)
+
+
+def _run(lib, sc, raw, ref_compat=True, rc_len=0, swst=None):
+    plan = asarf.FocusPlan(sc, lib=lib, ref_compat_stats=ref_compat, rc_fft_len=rc_len)
+    out = plan.focus_host(raw, swst)
+    return plan, out, plan.results()
+
+
+def _check(plan, out, res, ref):
+    assert res["errors"] == 0
+    assert res["first_line"] == ref.window["first_line"]
+    assert out.shape == ref.detected.shape
+    assert abs(res["dc_i"] - ref.iq.dc_i) <= 1e-6 * abs(ref.iq.dc_i)
+    assert abs(res["dc_q"] - ref.iq.dc_q) <= 1e-6 * abs(ref.iq.dc_q)
+    assert abs(res["iq_gain"] - ref.iq.iq_gain) <= 1e-6
+    assert abs(res["phase_error"] - ref.iq.phase_error) <= 1e-5
+    assert np.allclose(res["doppler_centroid_poly"][2], ref.dc_poly[2], rtol=1e-6, atol=1e-4)
+    assert rel_rmse(out, ref.detected) < TOL_DETECTED
+
+
+def test_tiny_matches_oracle(emu_lib):
+    sc, raw, _ = scene_and_raw(emu_lib, S.tiny)
+    plan, out, res = _run(emu_lib, sc, raw)
+    _check(plan, out, res, oracle_focus(sc, raw))
+
+
+def test_data_only_statistics(emu_lib):
+    """ref_compat_stats=False: gain/phase sums over the data block only (no padding bias)."""
+    sc, raw, _ = scene_and_raw(emu_lib, S.tiny)
+    plan, out, res = _run(emu_lib, sc, raw, ref_compat=False)
+    ref = oracle_focus(sc, raw, ref_compat=False)
+    _check(plan, out, res, ref)
+    assert abs(res["phase_error"]) < 5.0   # the true 2 deg skew, not the padding artefact
+
+
+def test_negative_doppler_window_variant(emu_lib):
+    """DC < 0 selects the other results-window variant (lines cut at the end)."""
+    sc, raw, _ = scene_and_raw(emu_lib, S.tiny, dc_coeffs=(-350.0,), seed=11)
+    plan, out, res = _run(emu_lib, sc, raw, ref_compat=False)
+    ref = oracle_focus(sc, raw, ref_compat=False)
+    assert ref.dc_poly[2] < 0 and res["variant"] == 1
+    _check(plan, out, res, ref)
+
+
+def test_range_fft_length_does_not_matter(emu_lib):
+    """Any range FFT length >= range size gives the same compressed samples."""
+    sc, raw, _ = scene_and_raw(emu_lib, S.tiny)
+    _, a, _ = _run(emu_lib, sc, raw, rc_len=768)
+    _, b, _ = _run(emu_lib, sc, raw, rc_len=1029)
+    assert rel_rmse(a, b) < 1e-5
+
+
+def test_swst_shift_and_unwindowed_chirp(emu_lib):
+    """Per-line SWST offsets (unfilled samples) and the unwindowed replica."""
+    na = 1024
+    codes = (np.arange(na) // 300 * 22 + 600).astype(np.uint16)  # ERS codes step by multiples of 22
+    sc, raw, _ = scene_and_raw(emu_lib, S.tiny, swst_codes=codes, range_size=768 + 4 * int(codes.max() - codes.min()),
+                               apply_window=False, seed=21)
+    plan = asarf.FocusPlan(sc, lib=emu_lib)
+    out = plan.focus_host(raw, codes)
+    res = plan.results()
+    ref = oracle_focus(sc, raw)
+    _check(plan, out, res, ref)
