@@ -266,7 +266,8 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
         // columns of this block beyond the data lie in the range padding (constant rows)
         int pad_lo = xb > a.nr ? xb : a.nr;
         int pad_hi = xe < a.rg_stride ? xe : a.rg_stride;
-        if (pad_hi > pad_lo) re += static_cast<double>(pad_hi - pad_lo) * (a.na - 1) * pad_mag2;
+        // (only when the padding went through the correction, i.e. reference statistics)
+        if (a.n_pad > 0 && pad_hi > pad_lo) re += static_cast<double>(pad_hi - pad_lo) * (a.na - 1) * pad_mag2;
         const double ang = atan2(im, re);
         const double hz = a.prf * (ang / (2.0 * 3.14159265358979323846));
         xs[b] = static_cast<double>((xb + xe) / 2);
@@ -408,6 +409,7 @@ ASARF_HD ASARF_INLINE ColParams az_col_params(const AzRdArgs& a, int x) {
     const float dc_steps = roundf(fdiv_rn(cp.dc, step));
     cp.dc_off = fmul_rn(dc_steps, step);
     cp.r0 = a.slant + static_cast<double>(x) * a.range_spacing;
+    cp.inv_dr = 1.0 / a.range_spacing;
     const float kav = fmul_rn(fmul_rn(2.0f, cp.vr), cp.vr);
     cp.ka = static_cast<float>(static_cast<double>(kav) / (static_cast<double>(a.lambda) * cp.r0));
     const float half = fmul_rn(a.prf, 0.5f);
@@ -438,7 +440,7 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
     const float den = fmul_rn(fmul_rn(8.0f, cp.vr), cp.vr);
     double dr = static_cast<double>(fdiv_rn(num, den));
     dr *= cp.r0;
-    const float shift = static_cast<float>(dr / a.range_spacing);
+    const float shift = static_cast<float>(dr * cp.inv_dr);
     const int walk = static_cast<int>(roundf(shift));
     const int calc_x = x + walk;
     float2 out = make_float2(0.0f, 0.0f);
@@ -449,6 +451,9 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
         } else {
             const float off = fadd_rn(fsub_rn(shift, static_cast<float>(walk)), static_cast<float>(kRcmcTaps / 2));
             const float pi = 3.14159265358979323846f;
+            // sin(pi (off - i)) = (-1)^i sin(pi off): one sinpi per output instead of one sinf per tap;
+            // the denominators pi (off - i) are rounded exactly as the reference rounds them
+            const float s_off = sinpi_f32(off);
             float si = 0.0f, sq = 0.0f, nrm = 0.0f;
 #pragma unroll
             for (int i = 0; i < kRcmcTaps; ++i) {
@@ -456,7 +461,7 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
                 float sinc = 1.0f;
                 if (arg != 0.0f) {
                     const float pa = fmul_rn(pi, arg);
-                    sinc = fdiv_rn(sinf(pa), pa);
+                    sinc = fmul_rn((i & 1) ? -s_off : s_off, rcp_f32(pa));
                 }
                 const float wgt = fmul_rn(ASARF_LDG(a.win + i), sinc);
                 const float2 d = srow[first + i];
@@ -464,7 +469,10 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
                 sq = fma_rn(d.y, wgt, sq);
                 nrm = fadd_rn(nrm, wgt);
             }
-            if (nrm != 0.0f) out = make_float2(fdiv_rn(si, nrm), fdiv_rn(sq, nrm));
+            if (nrm != 0.0f) {
+                const float inv = rcp_f32(nrm);
+                out = make_float2(fmul_rn(si, inv), fmul_rn(sq, inv));
+            }
         }
     }
     // --- azimuth matched filter

@@ -85,4 +85,22 @@ ASARF_HD ASARF_INLINE float fsub_rn(float a, float b) {
 #endif
 }
 
+// sin(pi x) with exact argument reduction (CUDA sinpif; FP64 on the host).
+ASARF_HD ASARF_INLINE float sinpi_f32(float x) {
+#if defined(__CUDA_ARCH__)
+    return sinpif(x);
+#else
+    return static_cast<float>(__builtin_sin(3.141592653589793238462643383279502884 * static_cast<double>(x)));
+#endif
+}
+
+// Correctly rounded reciprocal.
+ASARF_HD ASARF_INLINE float rcp_f32(float x) {
+#if defined(__CUDA_ARCH__)
+    return __frcp_rn(x);
+#else
+    return 1.0f / x;
+#endif
+}
+
 }  // namespace asarf

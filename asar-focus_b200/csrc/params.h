@@ -108,7 +108,7 @@ struct AzStridedArgs {
 
 struct ColParams {
     float dc, vr, dc_off, ka, cut_lo, cut_hi;
-    double r0;
+    double r0, inv_dr;
 };
 
 struct AzRdArgs {

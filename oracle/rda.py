@@ -163,11 +163,26 @@ def raw_data_correction(img: np.ndarray, x_size: int, y_size: int, n_total: int,
     delta = iq / i_sq2
     sin_c = F32(delta)
     cos_c = F32(1 - delta * delta)
-    q_new = (im - re * np.float64(sin_c)).astype(np.float32) / cos_c
+    q_new = fmaf(reg.real, -sin_c, reg.imag) / cos_c
     reg.imag[...] = q_new.astype(np.float32)
     phase_err = 360 * math.asin(delta) / (2 * math.pi)
     return IqResults(float(mean_i), float(mean_q), gain, phase_err, float(std_i), float(std_q),
                      float(sin_c), float(cos_c))
+
+
+def apply_iq_correction(block: np.ndarray, dc_i: float, dc_q: float, gain_f32: float, sin_c: float,
+                        cos_c: float) -> np.ndarray:
+    """The three correction kernels of RawDataCorrection on a complex64 block with given
+    float constants (sar/iq_correction.cu:140-178): I = (I - dc_i) / g; Q = fma(-I, s, Q - dc_q) / c.
+    NaN samples stay NaN."""
+    i1 = (block.real - F32(dc_i)).astype(np.float32)
+    q1 = (block.imag - F32(dc_q)).astype(np.float32)
+    i2 = (i1 / F32(gain_f32)).astype(np.float32)
+    q2 = fmaf(-i2, F32(sin_c), q1) / F32(cos_c)
+    out = np.empty_like(block)
+    out.real = i2
+    out.imag = q2.astype(np.float32)
+    return out
 
 
 def zero_nans(img: np.ndarray) -> None:

@@ -65,14 +65,17 @@ def test_range_fft_length_does_not_matter(emu_lib):
     assert rel_rmse(a, b) < 1e-5
 
 
-def test_swst_shift_and_unwindowed_chirp(emu_lib):
-    """Per-line SWST offsets (unfilled samples) and the unwindowed replica."""
+@pytest.mark.parametrize("ref_compat", [True, False])
+def test_swst_shift_and_unwindowed_chirp(emu_lib, ref_compat):
+    """Per-line SWST offsets (unfilled samples), a range size that is not a multiple of 32
+    (the last Doppler block runs into the range padding) and the unwindowed replica."""
     na = 1024
     codes = (np.arange(na) // 300 * 22 + 600).astype(np.uint16)  # ERS codes step by multiples of 22
     sc, raw, _ = scene_and_raw(emu_lib, S.tiny, swst_codes=codes, range_size=768 + 4 * int(codes.max() - codes.min()),
                                apply_window=False, seed=21)
-    plan = asarf.FocusPlan(sc, lib=emu_lib)
+    assert sc.range_size % 32 != 0
+    plan = asarf.FocusPlan(sc, lib=emu_lib, ref_compat_stats=ref_compat)
     out = plan.focus_host(raw, codes)
     res = plan.results()
-    ref = oracle_focus(sc, raw)
+    ref = oracle_focus(sc, raw, ref_compat=ref_compat)
     _check(plan, out, res, ref)
