@@ -54,6 +54,16 @@ class Results(C.Structure):
     ]
 
 
+class RawStats(C.Structure):
+    _fields_ = [
+        ("dc_i", C.c_double), ("dc_q", C.c_double), ("iq_gain", C.c_double), ("phase_error", C.c_double),
+        ("stddev_i", C.c_double), ("stddev_q", C.c_double), ("doppler_centroid_poly", C.c_double * 3),
+        ("n_dc_blocks", C.c_int32), ("reserved", C.c_int32), ("dc_block_hz", C.c_double * 80),
+        ("applied_dc_i", C.c_float), ("applied_dc_q", C.c_float), ("applied_gain", C.c_float),
+        ("applied_sin", C.c_float), ("applied_cos", C.c_float), ("errors", C.c_uint32),
+    ]
+
+
 class AsarfError(RuntimeError):
     pass
 
@@ -82,6 +92,9 @@ _SIGS = {
     "asarf_srgr_polynomial": (C.c_int, [C.POINTER(SceneC), C.c_double, C.c_int32, C.c_int32, C.c_double,
                                         C.POINTER(C.c_double * 5), C.POINTER(C.c_int32)]),
     "asarf_fft_size_above": (C.c_int32, [C.c_int32]),
+    "asarf_raw_statistics_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                               C.c_int32, C.c_int64, C.c_int32, C.c_double, C.c_void_p,
+                                               C.c_void_p]),
 }
 
 _cache: dict[str, C.CDLL] = {}

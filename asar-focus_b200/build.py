@@ -56,7 +56,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     objdir.mkdir(exist_ok=True)
     common = ["-std=c++17", "-O3", "-lineinfo", f"-I{INC}", f"-I{CSRC}", "-Xcompiler", "-fPIC"]
     objs = []
-    for src in ("kernels.cu", "host.cpp"):
+    for src in ("kernels.cu", "noalloc.cu", "host.cpp"):
         obj = objdir / (src + ".o")
         cmd = [NVCC, *GENCODE, *common, "-c", str(CSRC / src), "-o", str(obj)]
         if src.endswith(".cu") and verbose_ptxas:

@@ -87,6 +87,76 @@ int event_elapsed(void*, void*, float* ms) {
     return ASARF_OK;
 }
 size_t smem_optin_limit() { return 227 * 1024; }
+
+}  // namespace asarf
+
+// Host-emulation counterpart of noalloc.cu: the same bodies over a static host array.
+namespace {
+struct EmuNoallocScratch {
+    asarf::StatAccum acc;
+    asarf::FocusState state;
+};
+EmuNoallocScratch g_emu_scratch;
+}  // namespace
+
+extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_line_bytes, int32_t samples_per_line,
+                                            int32_t range_size, int32_t azimuth_size, const uint16_t* d_swst,
+                                            int32_t min_swst, int64_t total_raw_samples, int32_t stats_stride,
+                                            double prf, asarf_raw_stats* d_out, void*) {
+    using namespace asarf;
+    if (!d_raw || !d_out || range_size < 32 || azimuth_size < 2 || samples_per_line <= 0 ||
+        samples_per_line > range_size || (stats_stride != 0 && stats_stride < range_size))
+        return set_error(ASARF_ERR_INVALID, "raw_statistics_noalloc: bad arguments");
+    const int dc_step = range_size / 32;
+    const int nblk = (range_size + dc_step - 1) / dc_step;
+    if (nblk > kMaxDcBlocks) return set_error(ASARF_ERR_INVALID, "raw_statistics_noalloc: too many Doppler blocks");
+    std::memset(&g_emu_scratch.acc, 0, sizeof(StatAccum));
+    RawStatsArgs st{};
+    st.raw = d_raw;
+    st.line_bytes = raw_line_bytes;
+    st.spl = samples_per_line;
+    st.na = azimuth_size;
+    st.nr = range_size;
+    st.swst = d_swst;
+    st.min_swst = min_swst;
+    st.dc_step = dc_step;
+    st.nblk = nblk;
+    st.lines_per_cta = 64;
+    st.acc = &g_emu_scratch.acc;
+    backend_raw_stats(st, (range_size + 255) / 256, (azimuth_size + 63) / 64, 256, 256, nullptr);
+    FinalizeArgs fin{};
+    fin.acc = &g_emu_scratch.acc;
+    fin.state = &g_emu_scratch.state;
+    fin.n_total = total_raw_samples > 0 ? total_raw_samples : static_cast<long long>(samples_per_line) * azimuth_size;
+    const int stride = stats_stride > 0 ? stats_stride : range_size;
+    fin.n_pad = static_cast<long long>(stride - range_size) * azimuth_size;
+    fin.nr = range_size;
+    fin.na = azimuth_size;
+    fin.rg_stride = stride;
+    fin.dc_step = dc_step;
+    fin.nblk = nblk;
+    fin.prf = prf;
+    finalize_body(fin);
+    const FocusState& s = g_emu_scratch.state;
+    d_out->dc_i = s.dc_i_d;
+    d_out->dc_q = s.dc_q_d;
+    d_out->iq_gain = s.iq_gain;
+    d_out->phase_error = s.phase_error;
+    d_out->stddev_i = s.stddev_i;
+    d_out->stddev_q = s.stddev_q;
+    for (int k = 0; k < 3; ++k) d_out->doppler_centroid_poly[k] = s.dc_est[k];
+    d_out->n_dc_blocks = s.nblk;
+    for (int b = 0; b < kMaxDcBlocks; ++b) d_out->dc_block_hz[b] = b < s.nblk ? s.dc_blk_hz[b] : 0.0;
+    d_out->applied_dc_i = s.dc_i;
+    d_out->applied_dc_q = s.dc_q;
+    d_out->applied_gain = s.gain;
+    d_out->applied_sin = s.sin_c;
+    d_out->applied_cos = s.cos_c;
+    d_out->errors = s.errors;
+    return ASARF_OK;
+}
+
+namespace asarf {
 const char* backend_name() { return "host-emulation"; }
 
 }  // namespace asarf

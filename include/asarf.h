@@ -147,6 +147,40 @@ int asarf_plan_kernel_times(asarf_plan* plan, float* total_ms, int32_t* runs, co
 /* Results of the last run (synchronises `stream`). */
 int asarf_plan_results(asarf_plan* plan, asarf_results* res, void* stream);
 
+/* ---------------------------------------------------------------- allocation-free statistics */
+
+/* Output of asarf_raw_statistics_noalloc (written to device memory). */
+typedef struct asarf_raw_stats {
+    double dc_i, dc_q, iq_gain, phase_error, stddev_i, stddev_q;
+    double doppler_centroid_poly[3]; /* ACCC estimate, highest power first */
+    int32_t n_dc_blocks;
+    int32_t reserved;
+    double dc_block_hz[80];
+    float applied_dc_i, applied_dc_q, applied_gain, applied_sin, applied_cos;
+    uint32_t errors;
+} asarf_raw_stats;
+
+/* IQ statistics and Doppler-centroid estimate of device-resident raw ERS byte-I/Q data,
+ * taking no device memory at all.  This entry point has no counterpart in the reference.
+ *
+ * It is for callers that cannot call cudaMalloc: a check that runs while a CUDA graph is
+ * being captured, a host application whose own allocator owns all device memory, or a
+ * real-time ingest loop that cannot afford cudaMalloc's implicit synchronisation.  It
+ * computes what asarf_focus computes first (the statistics of RawDataCorrection and the
+ * estimate of CalculateDopplerCentroid) and writes them to `d_out`, a device buffer the
+ * caller owns.  Its only scratch is a fixed 8 KiB array in this library's static device
+ * memory, held on every GPU that loads the library until exit; it bounds the number of
+ * Doppler blocks to 80 (any range_size >= 32 gives 32 or 33) and larger counts are
+ * rejected with ASARF_ERR_INVALID.  All calls on a device share that array: calls whose
+ * work overlaps on the GPU race, so issue them in order on one stream.  The first call on
+ * each device looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  `stats_stride` is the padded width the reference runs
+ * its gain / phase sums over (its range FFT size; 0 = data samples only). */
+int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_line_bytes, int32_t samples_per_line,
+                                 int32_t range_size, int32_t azimuth_size, const uint16_t* d_swst, int32_t min_swst,
+                                 int64_t total_raw_samples, int32_t stats_stride, double prf, asarf_raw_stats* d_out,
+                                 void* stream);
+
 /* ---------------------------------------------------------------- host FP64 geometry */
 
 /* InterpolateOrbit (sar/orbit_state_vector.cc:23-48). */
