@@ -17,8 +17,9 @@ struct LaunchShape {
 int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, int threads, int cols, void* stream);
 int backend_finalize(const FinalizeArgs& a, void* stream);
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void* stream);
-int backend_az_strided(const AzStridedArgs& a, int tiles, int nblocks, LaunchShape sh, void* stream);
-int backend_az_rd(const AzRdArgs& a, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void* stream);
+int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream);
+int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, unsigned int* err,
+                  void* stream);
 int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err, void* stream);
 
 void* mem_alloc(size_t bytes);
@@ -35,6 +36,10 @@ int event_record(void* e, void* stream);
 int event_elapsed(void* a, void* b, float* ms);
 size_t smem_optin_limit();
 const char* backend_name();
+// Encode a float32 tiled tensor map (128-byte blob) of `rank` dims: dims[rank] innermost
+// first, strides[rank-1] in bytes, box[rank]; zero fill out of bounds.
+int backend_make_tmap(void* out, int rank, void* base, const unsigned long long* dims,
+                      const unsigned long long* strides, const unsigned int* box);
 
 // Records a message for asarf_last_error(); returns `code`.
 int set_error(int code, const char* fmt, ...);

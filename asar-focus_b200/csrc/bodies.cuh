@@ -307,11 +307,12 @@ ASARF_HD ASARF_INLINE float2 correct_sample(int iv, int qv, const FocusState& st
     return make_float2(i2, q2);
 }
 
-ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y, int tid, int nthr, float2* s) {
+ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y, int tid, int nthr, float2* s,
+                                               const uint8_t* raw_line) {
     const FocusState& st = *a.state;
     const int L = a.plan.n;
     const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
-    const uint8_t* row = a.raw + static_cast<long long>(y) * a.line_bytes;
+    const uint8_t* row = raw_line ? raw_line : a.raw + static_cast<long long>(y) * a.line_bytes;
     for (int l = tid; l < L; l += nthr) {
         float2 z = make_float2(0.0f, 0.0f);
         const int i = l - off;
@@ -335,24 +336,35 @@ ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y
 // [x0, x0 + xt).  Time index n = a*n2 + b, frequency k = k1 + n1*k2.
 //  forward (block b): Y[k1][b] = W_N^{b k1} * FFT_n1(x[a*n2 + b])[k1], stored at row k1*n2 + b.
 //  inverse (block b): x[a*n2 + b] = IFFT_n1(conj(W_N^{b k1}) * Z[k1][b])[a] * scale.
+// Both read their rows in natural order (one strided tile, TMA-loaded on the device) and
+// write the digit-reversed transform output straight to its destination rows.
 // Together with the contiguous pass this is the transpose-free equivalent of the reference's
 // transpose + batched row FFT + transpose (sar/range_doppler_algorithm.cu:314-326, 381-391).
-ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int b, int tid, int nthr, float2* s) {
+ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int b, int tid, int nthr, float2* s,
+                                           bool preloaded) {
     const int x0 = tile * a.xt;
     const int n1 = a.n1, xt = a.xt;
-    if (!a.inverse) {
+    const FastDiv dxt = make_fastdiv(static_cast<unsigned int>(xt));
+    // tile [r][c] = row r*n2 + b, column x0 + c (natural order; columns >= nk read as 0)
+    if (!preloaded) {
         for (int t = tid; t < n1 * xt; t += nthr) {
-            const int r = t / xt, c = t - r * xt;
+            const int r = static_cast<int>(fdiv_u(t, dxt)), c = t - r * xt;
             const int row = r * a.n2 + b;
             const int x = x0 + c;
             float2 v = make_float2(0.0f, 0.0f);
             if (row < a.valid_rows && x < a.nk) v = a.in[static_cast<long long>(row) * a.pitch + x];
             s[t] = v;
         }
-        ASARF_SYNC();
+    } else if (a.valid_rows < n1 * a.n2) {
+        // rows past the data hold stale values in memory: they are zero by definition
+        const int r0 = (a.valid_rows - b + a.n2 - 1) / a.n2;
+        for (int t = r0 * xt + tid; t < n1 * xt; t += nthr) s[t] = make_float2(0.0f, 0.0f);
+    }
+    ASARF_SYNC();
+    if (!a.inverse) {
         fft_forward(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
-            const int p = t / xt, c = t - p * xt;
+            const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
             const int k1 = ASARF_LDG(a.drev1 + p);
             const int x = x0 + c;
             if (x < a.nk) {
@@ -361,24 +373,17 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
             }
         }
     } else {
+        for (int t = tid; t < n1 * xt; t += nthr) {
+            const int k1 = static_cast<int>(fdiv_u(t, dxt));
+            s[t] = cmulc(s[t], ASARF_LDG(a.twn + b * k1));
+        }
+        ASARF_SYNC();
+        fft_inverse_dif(a.plan1, s, xt, xt, tid, nthr);
         const int lo = a.state ? a.state->first_line : 0;
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {
-            const int p = t / xt, c = t - p * xt;
-            const int k1 = ASARF_LDG(a.drev1 + p);
-            const int x = x0 + c;
-            float2 v = make_float2(0.0f, 0.0f);
-            if (x < a.nk) {
-                v = a.in[static_cast<long long>(k1 * a.n2 + b) * a.pitch + x];
-                v = cmulc(v, ASARF_LDG(a.twn + b * k1));
-            }
-            s[t] = v;
-        }
-        ASARF_SYNC();
-        fft_inverse(a.plan1, s, xt, xt, tid, nthr);
-        for (int t = tid; t < n1 * xt; t += nthr) {
-            const int r = t / xt, c = t - r * xt;
-            const int row = r * a.n2 + b;
+            const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
+            const int row = ASARF_LDG(a.drev1 + p) * a.n2 + b;
             const int x = x0 + c;
             if (x < a.nk && row >= lo && row < hi) {
                 const float2 v = s[t];
@@ -497,15 +502,19 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
 }
 
 ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s, float2* tmp,
-                                      ColParams* cps, unsigned int* err_flag) {
+                                      ColParams* cps, unsigned int* err_flag, bool preloaded) {
     const int x0 = tile * a.xt;
     const int n2 = a.n2, wt = a.wt;
-    for (int t = tid; t < n2 * wt; t += nthr) {
-        const int r = t / wt, c = t - r * wt;
-        const int x = x0 - a.hl + c;
-        float2 v = make_float2(0.0f, 0.0f);
-        if (x >= 0 && x < a.nk) v = a.in[static_cast<long long>(k1 * n2 + r) * a.pitch + x];
-        s[t] = v;
+    const FastDiv dwt = make_fastdiv(static_cast<unsigned int>(wt));
+    const FastDiv dxt = make_fastdiv(static_cast<unsigned int>(a.xt));
+    if (!preloaded) {
+        for (int t = tid; t < n2 * wt; t += nthr) {
+            const int r = static_cast<int>(fdiv_u(t, dwt)), c = t - r * wt;
+            const int x = x0 - a.hl + c;
+            float2 v = make_float2(0.0f, 0.0f);
+            if (x >= 0 && x < a.nk) v = a.in[static_cast<long long>(k1 * n2 + r) * a.pitch + x];
+            s[t] = v;
+        }
     }
     for (int c = tid; c < a.xt; c += nthr) cps[c] = az_col_params(a, x0 + c);
     ASARF_SYNC();
@@ -514,7 +523,7 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     for (int r0 = 0; r0 < n2; r0 += a.chunk_rows) {
         const int rn = (r0 + a.chunk_rows < n2) ? a.chunk_rows : n2 - r0;
         for (int t = tid; t < rn * a.xt; t += nthr) {
-            const int rr = t / a.xt, c = t - rr * a.xt;
+            const int rr = static_cast<int>(fdiv_u(t, dxt)), c = t - rr * a.xt;
             const int p = r0 + rr;
             const int x = x0 + c;
             float2 v = make_float2(0.0f, 0.0f);
@@ -526,14 +535,14 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
         }
         ASARF_SYNC();
         for (int t = tid; t < rn * a.xt; t += nthr) {
-            const int rr = t / a.xt, c = t - rr * a.xt;
+            const int rr = static_cast<int>(fdiv_u(t, dxt)), c = t - rr * a.xt;
             s[(r0 + rr) * wt + a.hl + c] = tmp[t];
         }
         ASARF_SYNC();
     }
     fft_inverse(a.plan2, s + a.hl, a.xt, wt, tid, nthr);
     for (int t = tid; t < n2 * a.xt; t += nthr) {
-        const int r = t / a.xt, c = t - r * a.xt;
+        const int r = static_cast<int>(fdiv_u(t, dxt)), c = t - r * a.xt;
         const int x = x0 + c;
         if (x < a.nk) a.out[static_cast<long long>(k1 * n2 + r) * a.pitch + x] = s[r * wt + a.hl + c];
     }

@@ -28,24 +28,24 @@ int backend_finalize(const FinalizeArgs& a, void*) {
 
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void*) {
     std::vector<float2> s(sh.smem / sizeof(float2) + 1);
-    for (int y = 0; y < lines; ++y) range_compress_body(a, y, 0, 1, s.data());
+    for (int y = 0; y < lines; ++y) range_compress_body(a, y, 0, 1, s.data(), nullptr);
     return ASARF_OK;
 }
 
-int backend_az_strided(const AzStridedArgs& a, int tiles, int nblocks, LaunchShape sh, void*) {
+int backend_az_strided(const AzStridedArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, void*) {
     std::vector<float2> s(sh.smem / sizeof(float2) + 1);
     for (int b = 0; b < nblocks; ++b)
-        for (int t = 0; t < tiles; ++t) az_strided_body(a, t, b, 0, 1, s.data());
+        for (int t = 0; t < tiles; ++t) az_strided_body(a, t, b, 0, 1, s.data(), false);
     return ASARF_OK;
 }
 
-int backend_az_rd(const AzRdArgs& a, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void*) {
+int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void*) {
     std::vector<float2> buf(sh.smem / sizeof(float2) + 16);
     float2* s = buf.data();
     float2* tmp = s + a.n2 * a.wt;
     ColParams* cps = reinterpret_cast<ColParams*>(tmp + a.chunk_rows * a.xt);
     for (int b = 0; b < nblocks; ++b)
-        for (int t = 0; t < tiles; ++t) az_rd_body(a, t, b, 0, 1, s, tmp, cps, err);
+        for (int t = 0; t < tiles; ++t) az_rd_body(a, t, b, 0, 1, s, tmp, cps, err, false);
     return ASARF_OK;
 }
 
@@ -158,5 +158,8 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
 
 namespace asarf {
 const char* backend_name() { return "host-emulation"; }
+int backend_make_tmap(void*, int, void*, const unsigned long long*, const unsigned long long*, const unsigned int*) {
+    return set_error(ASARF_ERR_INVALID, "no tensor maps in host emulation");
+}
 
 }  // namespace asarf

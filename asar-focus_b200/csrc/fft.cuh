@@ -30,6 +30,7 @@ struct FftPlan {
     int nst;
     int radix[kMaxStages];
     int span[kMaxStages];  // S of stage i (block length M = S * radix)
+    FastDiv sdiv[kMaxStages];
     const float2* tw;      // n entries
 };
 
@@ -165,21 +166,15 @@ ASARF_HD ASARF_INLINE void dft(float2* v) {
 // Forward (DIF): load R values at stride S, small DFT, multiply output q by W_M^{j q}.
 // Inverse (DIT): multiply input q by conj(W_M^{j q}), small inverse DFT.
 template <int R, bool INV>
-ASARF_HD ASARF_INLINE void fft_stage(float2* s, int n, int S, int ncol, int ldc, const float2* __restrict__ tw,
-                                          int tid, int nthr) {
+ASARF_HD ASARF_INLINE void fft_stage(float2* s, int n, int S, const FastDiv& sdiv, int ncol, const FastDiv& cdiv, int ldc,
+                                     const float2* __restrict__ tw, int tid, int nthr) {
     const int M = S * R;
     const int items = (n / R) * ncol;
     const int tw_step = n / M;
     for (int t = tid; t < items; t += nthr) {
-        int c, bj;
-        if (ncol == 1) {
-            c = 0;
-            bj = t;
-        } else {
-            bj = t / ncol;
-            c = t - bj * ncol;
-        }
-        const int b = bj / S;
+        const int bj = ncol == 1 ? t : static_cast<int>(fdiv_u(t, cdiv));
+        const int c = t - bj * ncol;
+        const int b = static_cast<int>(fdiv_u(bj, sdiv));
         const int j = bj - b * S;
         float2* p = s + (b * M + j) * ldc + c;
         const int st = S * ldc;
@@ -188,15 +183,59 @@ ASARF_HD ASARF_INLINE void fft_stage(float2* s, int n, int S, int ncol, int ldc,
         for (int m = 0; m < R; ++m) v[m] = p[m * st];
         if (INV) {
             if (j != 0) {
+                // W^{j q}: one table load, higher powers by recurrence (error ~ q ulp)
+                const float2 w1 = ASARF_LDG(tw + j * tw_step);
+                float2 w = w1;
 #pragma unroll
-                for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], ASARF_LDG(tw + j * q * tw_step));
+                for (int q = 1; q < R; ++q) {
+                    v[q] = cmulc(v[q], w);
+                    w = cmul(w, w1);
+                }
             }
             dft<R, true>(v);
         } else {
             dft<R, false>(v);
             if (j != 0) {
+                const float2 w1 = ASARF_LDG(tw + j * tw_step);
+                float2 w = w1;
 #pragma unroll
-                for (int q = 1; q < R; ++q) v[q] = cmul(v[q], ASARF_LDG(tw + j * q * tw_step));
+                for (int q = 1; q < R; ++q) {
+                    v[q] = cmul(v[q], w);
+                    w = cmul(w, w1);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) p[m * st] = v[m];
+    }
+}
+
+// Inverse transform in decimation-in-frequency form: small inverse DFT, then multiply output
+// q by conj(W_M^{j q}).  Natural-order input, digit-reversed output (same map as the forward).
+template <int R>
+ASARF_HD ASARF_INLINE void fft_stage_dif_inv(float2* s, int n, int S, const FastDiv& sdiv, int ncol, const FastDiv& cdiv,
+                                             int ldc, const float2* __restrict__ tw, int tid, int nthr) {
+    const int M = S * R;
+    const int items = (n / R) * ncol;
+    const int tw_step = n / M;
+    for (int t = tid; t < items; t += nthr) {
+        const int bj = ncol == 1 ? t : static_cast<int>(fdiv_u(t, cdiv));
+        const int c = t - bj * ncol;
+        const int b = static_cast<int>(fdiv_u(bj, sdiv));
+        const int j = bj - b * S;
+        float2* p = s + (b * M + j) * ldc + c;
+        const int st = S * ldc;
+        float2 v[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[m] = p[m * st];
+        dft<R, true>(v);
+        if (j != 0) {
+            const float2 w1 = ASARF_LDG(tw + j * tw_step);
+            float2 w = w1;
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                v[q] = cmulc(v[q], w);
+                w = cmul(w, w1);
             }
         }
 #pragma unroll
@@ -205,31 +244,51 @@ ASARF_HD ASARF_INLINE void fft_stage(float2* s, int n, int S, int ncol, int ldc,
 }
 
 template <bool INV>
-ASARF_HD ASARF_INLINE void fft_stage_dispatch(int R, float2* s, int n, int S, int ncol, int ldc,
-                                                   const float2* __restrict__ tw, int tid, int nthr) {
+ASARF_HD ASARF_INLINE void fft_stage_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int ncol,
+                                              const FastDiv& cdiv, int ldc, const float2* __restrict__ tw, int tid,
+                                              int nthr) {
     switch (R) {
-        case 2: fft_stage<2, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
-        case 3: fft_stage<3, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
-        case 4: fft_stage<4, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
-        case 5: fft_stage<5, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
-        case 7: fft_stage<7, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
-        default: fft_stage<8, INV>(s, n, S, ncol, ldc, tw, tid, nthr); break;
+        case 2: fft_stage<2, INV>(s, n, S, sdiv, ncol, cdiv, ldc, tw, tid, nthr); break;
+        case 3: fft_stage<3, INV>(s, n, S, sdiv, ncol, cdiv, ldc, tw, tid, nthr); break;
+        case 4: fft_stage<4, INV>(s, n, S, sdiv, ncol, cdiv, ldc, tw, tid, nthr); break;
+        case 5: fft_stage<5, INV>(s, n, S, sdiv, ncol, cdiv, ldc, tw, tid, nthr); break;
+        case 7: fft_stage<7, INV>(s, n, S, sdiv, ncol, cdiv, ldc, tw, tid, nthr); break;
+        default: fft_stage<8, INV>(s, n, S, sdiv, ncol, cdiv, ldc, tw, tid, nthr); break;
     }
 }
 
 // Forward DIF transform of ncol independent columns; output digit-reversed.  The caller
 // places a barrier after loading the tile; this returns after a final barrier.
 ASARF_HD ASARF_INLINE void fft_forward(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    const FastDiv cdiv = make_fastdiv(static_cast<unsigned int>(ncol));
     for (int i = 0; i < p.nst; ++i) {
-        fft_stage_dispatch<false>(p.radix[i], s, p.n, p.span[i], ncol, ldc, p.tw, tid, nthr);
+        fft_stage_dispatch<false>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], ncol, cdiv, ldc, p.tw, tid, nthr);
         ASARF_SYNC();
     }
 }
 
 // Inverse DIT transform (digit-reversed input, natural output, unscaled).
 ASARF_HD ASARF_INLINE void fft_inverse(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    const FastDiv cdiv = make_fastdiv(static_cast<unsigned int>(ncol));
     for (int i = p.nst - 1; i >= 0; --i) {
-        fft_stage_dispatch<true>(p.radix[i], s, p.n, p.span[i], ncol, ldc, p.tw, tid, nthr);
+        fft_stage_dispatch<true>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], ncol, cdiv, ldc, p.tw, tid, nthr);
+        ASARF_SYNC();
+    }
+}
+
+// Inverse transform, natural-order input, digit-reversed output, unscaled.
+ASARF_HD ASARF_INLINE void fft_inverse_dif(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    const FastDiv cdiv = make_fastdiv(static_cast<unsigned int>(ncol));
+    for (int i = 0; i < p.nst; ++i) {
+        const FastDiv& sd = p.sdiv[i];
+        switch (p.radix[i]) {
+            case 2: fft_stage_dif_inv<2>(s, p.n, p.span[i], sd, ncol, cdiv, ldc, p.tw, tid, nthr); break;
+            case 3: fft_stage_dif_inv<3>(s, p.n, p.span[i], sd, ncol, cdiv, ldc, p.tw, tid, nthr); break;
+            case 4: fft_stage_dif_inv<4>(s, p.n, p.span[i], sd, ncol, cdiv, ldc, p.tw, tid, nthr); break;
+            case 5: fft_stage_dif_inv<5>(s, p.n, p.span[i], sd, ncol, cdiv, ldc, p.tw, tid, nthr); break;
+            case 7: fft_stage_dif_inv<7>(s, p.n, p.span[i], sd, ncol, cdiv, ldc, p.tw, tid, nthr); break;
+            default: fft_stage_dif_inv<8>(s, p.n, p.span[i], sd, ncol, cdiv, ldc, p.tw, tid, nthr); break;
+        }
         ASARF_SYNC();
     }
 }

@@ -85,6 +85,36 @@ ASARF_HD ASARF_INLINE float fsub_rn(float a, float b) {
 #endif
 }
 
+// Division by a loop-invariant divisor d < 2^16 of n < 2^16 without a hardware divide:
+// q = umulhi(n, ceil(2^32 / d)) (exact while n * (m d - 2^32) < 2^32), or a shift when d is
+// a power of two.
+struct FastDiv {
+    unsigned int d;
+    unsigned int m;      // 0: power of two, use shift
+    unsigned int shift;
+};
+
+ASARF_HD ASARF_INLINE FastDiv make_fastdiv(unsigned int d) {
+    FastDiv f{d, 0u, 0u};
+    if ((d & (d - 1)) == 0) {
+        unsigned int s = 0;
+        while ((1u << s) < d) ++s;
+        f.shift = s;
+    } else {
+        f.m = static_cast<unsigned int>((0x100000000ull + d - 1) / d);
+    }
+    return f;
+}
+
+ASARF_HD ASARF_INLINE unsigned int fdiv_u(unsigned int n, const FastDiv& f) {
+    if (f.m == 0) return n >> f.shift;
+#if defined(__CUDA_ARCH__)
+    return __umulhi(n, f.m);
+#else
+    return static_cast<unsigned int>((static_cast<unsigned long long>(n) * f.m) >> 32);
+#endif
+}
+
 // sin(pi x) with exact argument reduction (CUDA sinpif; FP64 on the host).
 ASARF_HD ASARF_INLINE float sinpi_f32(float x) {
 #if defined(__CUDA_ARCH__)

@@ -305,6 +305,7 @@ static bool build_fft(int n, HostFft& h) {
     for (size_t i = 0; i < f.size(); ++i) {
         h.plan.radix[i] = f[i];
         h.plan.span[i] = M / f[i];
+        h.plan.sdiv[i] = make_fastdiv(static_cast<unsigned int>(M / f[i]));
         spans.push_back(M / f[i]);
         M /= f[i];
     }
@@ -383,6 +384,12 @@ struct asarf_plan {
     // optional per-kernel timing (events recorded between the launches of each run)
     std::vector<void*> events;
     int timing_slots = 0, timing_used = 0;
+    // TMA tensor maps (device build): strided views of A and B, contiguous view of A
+    alignas(64) unsigned char tmapA3[128] = {};
+    alignas(64) unsigned char tmapB3[128] = {};
+    alignas(64) unsigned char tmapA2[128] = {};
+    bool use_tma = false;
+    int raw_smem_offset = 0;
 
     template <class T>
     T* alloc(size_t count) {
@@ -557,6 +564,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         const double walk = s.wavelength * s.wavelength * f * f * rmax / (8 * vr_min * vr_min) / s.range_spacing;
         p->hl = kRcmcTaps / 2;
         p->hr = kRcmcTaps / 2 + static_cast<int>(std::ceil(walk)) + 2;
+        if ((32 + p->hl + p->hr) & 1) ++p->hr;  // even tile width: TMA rows are whole 16-byte units
     }
     p->pitch = (p->nk + 31) / 32 * 32;
     p->xt1 = (p->n1 * 32 * 8 <= 160 * 1024) ? 32 : 16;
@@ -722,7 +730,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     r.nk = p->nk;
     r.out = p->bufA;
     r.out_pitch = p->pitch;
-    p->sh_rc = {256, sizeof(float2) * static_cast<size_t>(p->rc_len)};
+    p->raw_smem_offset = static_cast<int>((sizeof(float2) * static_cast<size_t>(p->rc_len) + 127) / 128 * 128);
+    p->sh_rc = {512, static_cast<size_t>(p->raw_smem_offset) + (2 * static_cast<size_t>(s.samples_per_line) + 15) / 16 * 16};
 
     AzStridedArgs& f = p->a_fwd;
     f.in = p->bufA;
@@ -736,7 +745,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     f.nk = p->nk;
     f.xt = p->xt1;
     f.valid_rows = p->na;
-    f.state = nullptr;
+    f.state = p->state;
     f.scale = 1.0f;
     f.inverse = 0;
     p->a_inv = f;
@@ -794,6 +803,32 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     t.ground_spacing = kGroundSpacing;
     t.out_pitch = p->out_cols_max;
     p->sh_tail = {256, sizeof(float) * static_cast<size_t>(p->nx)};
+
+    // ---- TMA tensor maps (all tiles come from this GPU's own buffers; loads only)
+    {
+        auto largest_divisor_le = [](int n, int cap) {
+            for (int d = std::min(n, cap); d >= 1; --d)
+                if (n % d == 0) return d;
+            return 1;
+        };
+        const int n1_box = largest_divisor_le(p->n1, 256);
+        const int n2_box = largest_divisor_le(p->n2, 256);
+        const unsigned long long row_bytes = static_cast<unsigned long long>(p->pitch) * sizeof(float2);
+        const unsigned long long d3[3] = {2ull * p->nk, static_cast<unsigned long long>(p->n2),
+                                          static_cast<unsigned long long>(p->n1)};
+        const unsigned long long s3[2] = {row_bytes, row_bytes * p->n2};
+        const unsigned int b3[3] = {static_cast<unsigned int>(2 * p->xt1), 1u, static_cast<unsigned int>(n1_box)};
+        const unsigned long long d2[2] = {2ull * p->nk, static_cast<unsigned long long>(p->az_pad)};
+        const unsigned long long s2[1] = {row_bytes};
+        const unsigned int b2[2] = {static_cast<unsigned int>(2 * d.wt), static_cast<unsigned int>(n2_box)};
+        const bool shapes_ok = (d.wt % 2 == 0) && 2 * d.wt <= 256 && 2 * p->xt1 <= 256;
+        p->use_tma = shapes_ok && backend_make_tmap(p->tmapA3, 3, p->bufA, d3, s3, b3) == ASARF_OK &&
+                     backend_make_tmap(p->tmapB3, 3, p->bufB, d3, s3, b3) == ASARF_OK &&
+                     backend_make_tmap(p->tmapA2, 2, p->bufA, d2, s2, b2) == ASARF_OK;
+        p->a_fwd.use_tma = p->a_inv.use_tma = d.use_tma = p->use_tma ? 1 : 0;
+        p->a_fwd.n1_box = p->a_inv.n1_box = n1_box;
+        d.n2_box = n2_box;
+    }
 
     const size_t lim = smem_optin_limit();
     if (p->sh_rc.smem > lim || p->sh_st.smem > lim || p->sh_rd.smem > lim || p->sh_tail.smem > lim) {
@@ -866,17 +901,21 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     r.raw = d_raw;
     r.swst = d_swst;
     r.min_swst = min_swst;
+    const bool aligned = (reinterpret_cast<uintptr_t>(d_raw) % 16 == 0) && (p->scene.raw_line_bytes % 16 == 0);
+    r.bulk_bytes = (p->use_tma && aligned) ? (2 * p->scene.samples_per_line) / 16 * 16 : 0;
+    r.raw_smem_offset = p->raw_smem_offset;
     mark();
     rc = backend_range_compress(r, p->na, p->sh_rc, stream);
     if (rc) return rc;
     mark();
-    rc = backend_az_strided(p->a_fwd, p->tiles1, p->n2, p->sh_st, stream);
+    rc = backend_az_strided(p->a_fwd, p->use_tma ? p->tmapA3 : nullptr, p->tiles1, p->n2, p->sh_st, stream);
     if (rc) return rc;
     mark();
-    rc = backend_az_rd(p->a_rd, p->tiles2, p->n1, p->sh_rd, &p->state->errors, stream);
+    rc = backend_az_rd(p->a_rd, p->use_tma ? p->tmapA2 : nullptr, p->tiles2, p->n1, p->sh_rd, &p->state->errors,
+                       stream);
     if (rc) return rc;
     mark();
-    rc = backend_az_strided(p->a_inv, p->tiles1, p->n2, p->sh_st, stream);
+    rc = backend_az_strided(p->a_inv, p->use_tma ? p->tmapB3 : nullptr, p->tiles1, p->n2, p->sh_st, stream);
     if (rc) return rc;
     TailArgs t = p->a_tail;
     t.out = d_out;

@@ -2,10 +2,15 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstring>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "asarf.h"
 #include "backend.h"
 #include "bodies.cuh"
+#include "tma.cuh"
 
 namespace asarf {
 
@@ -20,23 +25,69 @@ __global__ void k_finalize(FinalizeArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) finalize_body(a);
 }
 
+// One raw line per block; with bulk_bytes > 0 thread 0 fetches the line with one bulk copy
+// into shared memory (the sub-16-byte tail with plain loads) while the others wait.
 __global__ void __launch_bounds__(512) k_range_compress(RangeCompressArgs a) {
-    extern __shared__ float2 smem_rc[];
-    range_compress_body(a, blockIdx.x, threadIdx.x, blockDim.x, smem_rc);
+    extern __shared__ __align__(1024) unsigned char smem_rc_raw[];
+    float2* s = reinterpret_cast<float2*>(smem_rc_raw);
+    __shared__ uint64_t bar;
+    const uint8_t* line = nullptr;
+    if (a.bulk_bytes > 0) {
+        uint8_t* buf = smem_rc_raw + a.raw_smem_offset;
+        const uint8_t* src = a.raw + static_cast<long long>(blockIdx.x) * a.line_bytes;
+        const int total = 2 * a.spl;
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, static_cast<uint32_t>(a.bulk_bytes));
+            bulk_load(buf, src, static_cast<uint32_t>(a.bulk_bytes), &bar);
+        }
+        for (int i = a.bulk_bytes + threadIdx.x; i < total; i += blockDim.x) buf[i] = src[i];
+        __syncthreads();
+        mbar_wait(&bar, 0, &const_cast<FocusState*>(a.state)->errors);
+        line = buf;
+    }
+    range_compress_body(a, blockIdx.x, threadIdx.x, blockDim.x, s, line);
 }
 
-__global__ void __launch_bounds__(512) k_az_strided(AzStridedArgs a) {
-    extern __shared__ float2 smem_as[];
-    az_strided_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, smem_as);
+// Strided azimuth pass: the [n1][xt] tile (rows r*n2 + b) arrives by 3-D TMA boxes.
+__global__ void __launch_bounds__(512) k_az_strided(AzStridedArgs a, const __grid_constant__ CUtensorMap map) {
+    extern __shared__ __align__(1024) unsigned char smem_as_raw[];
+    float2* s = reinterpret_cast<float2*>(smem_as_raw);
+    __shared__ uint64_t bar;
+    if (a.use_tma) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, static_cast<uint32_t>(sizeof(float2) * a.n1 * a.xt));
+            for (int r0 = 0; r0 < a.n1; r0 += a.n1_box)
+                tma_load_3d(s + static_cast<size_t>(r0) * a.xt, &map, &bar, 2 * blockIdx.x * a.xt, blockIdx.y, r0);
+        }
+        __syncthreads();
+        mbar_wait(&bar, 0, a.state ? &const_cast<FocusState*>(a.state)->errors : nullptr);
+    }
+    az_strided_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, a.use_tma != 0);
 }
 
-__global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err) {
-    extern __shared__ float2 smem_rd[];
+// Range-Doppler block: the [n2][wt] tile (contiguous rows, range halo) arrives by 2-D TMA
+// boxes; columns left of 0 and right of nk are filled with zeros by the TMA unit.
+__global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, const __grid_constant__ CUtensorMap map) {
+    extern __shared__ __align__(1024) unsigned char smem_rd_raw[];
     const int wt = a.wt;
-    float2* s = smem_rd;
+    float2* s = reinterpret_cast<float2*>(smem_rd_raw);
     float2* tmp = s + a.n2 * wt;
     ColParams* cps = reinterpret_cast<ColParams*>(tmp + a.chunk_rows * a.xt);
-    az_rd_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, tmp, cps, err);
+    __shared__ uint64_t bar;
+    if (a.use_tma) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, static_cast<uint32_t>(sizeof(float2) * a.n2 * wt));
+            const int x = 2 * (static_cast<int>(blockIdx.x) * a.xt - a.hl);
+            for (int r0 = 0; r0 < a.n2; r0 += a.n2_box)
+                tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
+        }
+        __syncthreads();
+        mbar_wait(&bar, 0, err);
+    }
+    az_rd_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, tmp, cps, err, a.use_tma != 0);
 }
 
 __global__ void __launch_bounds__(512) k_tail(TailArgs a, unsigned int* err) {
@@ -80,18 +131,56 @@ int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh
     return check_launch("range_compress");
 }
 
-int backend_az_strided(const AzStridedArgs& a, int tiles, int nblocks, LaunchShape sh, void* stream) {
+static CUtensorMap tmap_or_zero(const void* tmap) {
+    CUtensorMap m;
+    if (tmap)
+        std::memcpy(&m, tmap, sizeof(m));
+    else
+        std::memset(&m, 0, sizeof(m));
+    return m;
+}
+
+int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream) {
     int rc = ensure_smem(k_az_strided, sh.smem, "az_strided");
     if (rc) return rc;
-    k_az_strided<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a);
+    k_az_strided<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, tmap_or_zero(tmap));
     return check_launch("az_strided");
 }
 
-int backend_az_rd(const AzRdArgs& a, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void* stream) {
+int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, unsigned int* err,
+                  void* stream) {
     int rc = ensure_smem(k_az_rd, sh.smem, "az_rd");
     if (rc) return rc;
-    k_az_rd<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, err);
+    k_az_rd<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, err, tmap_or_zero(tmap));
     return check_launch("az_rd");
+}
+
+int backend_make_tmap(void* out, int rank, void* base, const unsigned long long* dims,
+                      const unsigned long long* strides, const unsigned int* box) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            return set_error(ASARF_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    cuuint64_t gdim[5], gstr[4];
+    cuuint32_t bdim[5], estr[5];
+    for (int i = 0; i < rank; ++i) {
+        gdim[i] = dims[i];
+        bdim[i] = box[i];
+        estr[i] = 1;
+    }
+    for (int i = 0; i + 1 < rank; ++i) gstr[i] = strides[i];
+    CUresult r = encode(static_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, base, gdim, gstr, bdim,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(ASARF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", static_cast<int>(r));
+    return ASARF_OK;
 }
 
 int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err, void* stream) {

@@ -88,6 +88,8 @@ struct RangeCompressArgs {
     int nk;
     float2* out;
     long long out_pitch;
+    int bulk_bytes;       // raw bytes per line fetched by one bulk copy (multiple of 16; 0 = plain loads)
+    int raw_smem_offset;  // byte offset of the raw-line buffer in shared memory
 };
 
 struct AzStridedArgs {
@@ -104,6 +106,8 @@ struct AzStridedArgs {
     const FocusState* state;  // inverse: rows outside the results window are not stored
     float scale;          // inverse: 1 / N as the reference multiplies
     int inverse;
+    int use_tma;          // tile loaded by TMA (device only)
+    int n1_box;           // rows per TMA box (n1 split into n1 / n1_box boxes of <= 256 rows)
 };
 
 struct ColParams {
@@ -126,6 +130,8 @@ struct AzRdArgs {
     float vr_poly[3];
     const FocusState* state;
     const float* win;     // 16 RCMC window taps
+    int use_tma;
+    int n2_box;           // rows per TMA box
 };
 
 struct TailVariant {
