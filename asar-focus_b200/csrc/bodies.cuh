@@ -105,55 +105,98 @@ ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by,
     const int y0 = by * a.lines_per_cta;
     const int y1 = (y0 + a.lines_per_cta < a.na) ? y0 + a.lines_per_cta : a.na;
     const int ys = y0 > 0 ? y0 - 1 : 0;
-    for (int t = tid; t < cols; t += nthr) {
-        const int x = bx * cols + t;
-        const bool xin = x < a.nr;
-        unsigned long long cnt = 0, si = 0, sq = 0, sii = 0, sqq = 0, siq = 0;
-        unsigned int l[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        int pi = 0, pq = 0;
-        bool pf = false;
+    const FastDiv dstep = make_fastdiv(static_cast<unsigned int>(a.dc_step));
+    // thread item t covers columns x = bx*cols + 4t .. +3 (cols is a multiple of 4*nthr)
+    for (int t = tid; t < cols / 4; t += nthr) {
+        const int xb = bx * cols + 4 * t;
+        const bool xin = xb < a.nr;
+        unsigned int cnt = 0, si = 0, sq = 0, sii = 0, sqq = 0, siq = 0;
+        unsigned int l[4][9];
+        for (int k = 0; k < 4; ++k)
+            for (int q = 0; q < 9; ++q) l[k][q] = 0u;
+        int pi[4] = {0, 0, 0, 0}, pq[4] = {0, 0, 0, 0};
+        bool pf[4] = {false, false, false, false};
         if (xin) {
             for (int y = ys; y < y1; ++y) {
                 const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
-                const int i = x - off;
-                const bool f = (i >= 0) && (i < a.spl);
-                int iv = 0, qv = 0;
-                if (f) {
-                    const uint16_t w = *reinterpret_cast<const uint16_t*>(a.raw + static_cast<long long>(y) * a.line_bytes +
-                                                                          2ll * i);
-                    iv = w & 0xff;
-                    qv = w >> 8;
+                const int i0 = xb - off;
+                const uint8_t* rowp = a.raw + static_cast<long long>(y) * a.line_bytes;
+                int iv[4], qv[4];
+                bool f[4];
+                if (a.vec_ok && i0 >= 0 && i0 + 4 <= a.spl && xb + 4 <= a.nr) {
+                    const uint2 w = *reinterpret_cast<const uint2*>(rowp + 2ll * i0);
+                    iv[0] = w.x & 0xff;
+                    qv[0] = (w.x >> 8) & 0xff;
+                    iv[1] = (w.x >> 16) & 0xff;
+                    qv[1] = w.x >> 24;
+                    iv[2] = w.y & 0xff;
+                    qv[2] = (w.y >> 8) & 0xff;
+                    iv[3] = (w.y >> 16) & 0xff;
+                    qv[3] = w.y >> 24;
+                    f[0] = f[1] = f[2] = f[3] = true;
+                } else {
+                    for (int k = 0; k < 4; ++k) {
+                        const int i = i0 + k;
+                        f[k] = (xb + k < a.nr) && (i >= 0) && (i < a.spl);
+                        iv[k] = qv[k] = 0;
+                        if (f[k]) {
+                            const uint16_t w = *reinterpret_cast<const uint16_t*>(rowp + 2ll * i);
+                            iv[k] = w & 0xff;
+                            qv[k] = w >> 8;
+                        }
+                    }
                 }
                 if (y >= y0) {
-                    if (f) {
-                        cnt += 1;
-                        si += iv;
-                        sq += qv;
-                        sii += iv * iv;
-                        sqq += qv * qv;
-                        siq += iv * qv;
-                    }
-                    if (y > 0 && f && pf) {
-                        l[0] += 1;
-                        l[1] += pi;
-                        l[2] += pq;
-                        l[3] += iv;
-                        l[4] += qv;
-                        l[5] += pi * iv;
-                        l[6] += pq * qv;
-                        l[7] += pi * qv;
-                        l[8] += pq * iv;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (f[k]) {
+                            cnt += 1;
+                            si += iv[k];
+                            sq += qv[k];
+                            sii += iv[k] * iv[k];
+                            sqq += qv[k] * qv[k];
+                            siq += iv[k] * qv[k];
+                        }
+                        if (y > 0 && f[k] && pf[k]) {
+                            l[k][0] += 1;
+                            l[k][1] += pi[k];
+                            l[k][2] += pq[k];
+                            l[k][3] += iv[k];
+                            l[k][4] += qv[k];
+                            l[k][5] += pi[k] * iv[k];
+                            l[k][6] += pq[k] * qv[k];
+                            l[k][7] += pi[k] * qv[k];
+                            l[k][8] += pq[k] * iv[k];
+                        }
                     }
                 }
-                pi = iv;
-                pq = qv;
-                pf = f;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    pi[k] = iv[k];
+                    pq[k] = qv[k];
+                    pf[k] = f[k];
+                }
+            }
+        }
+        // the four columns belong to at most two Doppler blocks (blocks are >= 4 columns wide)
+        const int b_first = xin ? static_cast<int>(fdiv_u(xb, dstep)) : 0;
+        unsigned int la[9], lb[9];
+        int b_second = b_first;
+        for (int q = 0; q < 9; ++q) la[q] = lb[q] = 0u;
+        for (int k = 0; k < 4; ++k) {
+            const int x = xb + k;
+            if (!xin || x >= a.nr) continue;
+            const int bk = static_cast<int>(fdiv_u(x, dstep));
+            if (bk == b_first) {
+                for (int q = 0; q < 9; ++q) la[q] += l[k][q];
+            } else {
+                b_second = bk;
+                for (int q = 0; q < 9; ++q) lb[q] += l[k][q];
             }
         }
         unsigned long long mv[6] = {cnt, si, sq, sii, sqq, siq};
-        const int blk = xin ? x / a.dc_step : 0;
 #if defined(__CUDA_ARCH__)
-        // warp reduction first: all lanes run this loop iteration (cols is a multiple of nthr)
+        // warp reductions first: all lanes run this loop iteration (cols is a multiple of 4*nthr)
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             unsigned long long v = mv[k];
@@ -164,27 +207,27 @@ ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by,
 #pragma unroll
             for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
         }
-        const int bmin = __reduce_min_sync(0xffffffffu, xin ? blk : 0x7fffffff);
-        const int bmax = __reduce_max_sync(0xffffffffu, xin ? blk : -1);
-        if (bmin == bmax) {
+        const bool single = !xin || b_second == b_first;
+        const int bmin = __reduce_min_sync(0xffffffffu, xin ? b_first : 0x7fffffff);
+        const int bmax = __reduce_max_sync(0xffffffffu, xin ? b_first : -1);
+        const bool uniform = __all_sync(0xffffffffu, single) && bmin == bmax;
+        if (uniform) {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                unsigned int v = xin ? l[k] : 0u;
-                v = __reduce_add_sync(0xffffffffu, v);
-                l[k] = v;
-            }
-            if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-                for (int k = 0; k < 9; ++k) atomic_add_u64(&sm->lag[bmin][k], l[k]);
-            }
+            for (int q = 0; q < 9; ++q) la[q] = __reduce_add_sync(0xffffffffu, xin ? la[q] : 0u);
+            if ((threadIdx.x & 31) == 0)
+                for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[bmin][q], la[q]);
         } else if (xin) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) atomic_add_u64(&sm->lag[blk][k], l[k]);
+            for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_first][q], la[q]);
+            if (b_second != b_first)
+                for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_second][q], lb[q]);
         }
 #else
         for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
-        if (xin)
-            for (int k = 0; k < 9; ++k) atomic_add_u64(&sm->lag[blk][k], l[k]);
+        if (xin) {
+            for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_first][q], la[q]);
+            if (b_second != b_first)
+                for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_second][q], lb[q]);
+        }
 #endif
     }
     ASARF_SYNC();
@@ -410,7 +453,7 @@ ASARF_HD ASARF_INLINE ColParams az_col_params(const AzRdArgs& a, int x) {
     float vrp[3] = {a.vr_poly[0], a.vr_poly[1], a.vr_poly[2]};
     cp.dc = polyval_f32(dcp, xf);
     cp.vr = polyval_f32(vrp, xf);
-    const float step = fdiv_rn(a.prf, static_cast<float>(a.az_pad));
+    const float step = a.bin_step;
     const float dc_steps = roundf(fdiv_rn(cp.dc, step));
     cp.dc_off = fmul_rn(dc_steps, step);
     cp.r0 = a.slant + static_cast<double>(x) * a.range_spacing;
@@ -420,6 +463,8 @@ ASARF_HD ASARF_INLINE ColParams az_col_params(const AzRdArgs& a, int x) {
     const float half = fmul_rn(a.prf, 0.5f);
     cp.cut_hi = fma_rn(half, a.frac, cp.dc_off);
     cp.cut_lo = fma_rn(-half, a.frac, cp.dc_off);
+    cp.den = fmul_rn(fmul_rn(8.0f, cp.vr), cp.vr);
+    cp.dc_off_ka = fdiv_rn(cp.dc_off, cp.ka);
     return cp;
 }
 
@@ -428,12 +473,29 @@ ASARF_HD ASARF_INLINE float bin_frequency(int f, int az_pad, float step) {
     return fmul_rn(static_cast<float>(k), step);
 }
 
+// Approximate quotient (2 ulp) for the interpolation weights, whose rounding never reaches a
+// branch: one reciprocal-multiply on the device.
+ASARF_HD ASARF_INLINE float fast_div(float a, float b) {
+#if defined(__CUDA_ARCH__)
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+
 ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& cp, int x, int f, const float2* srow,
                                             int cs, unsigned int* err_flag) {
     const float prf = a.prf;
-    const float step = fdiv_rn(prf, static_cast<float>(a.az_pad));
-    const float half = fmul_rn(prf, 0.5f);
-    const float bf = bin_frequency(f, a.az_pad, step);
+    const float half = a.half_prf;
+    const float bf = bin_frequency(f, a.az_pad, a.bin_step);
+    // --- azimuth matched filter band: outside it the reference writes zero whatever RCMC gave
+    float absf = bf;
+    if (cp.dc < 0.0f) {
+        if (bf > fadd_rn(half, cp.dc)) absf = fsub_rn(absf, prf);
+    } else if (cp.dc > 0.0f) {
+        if (absf < fadd_rn(-half, cp.dc)) absf = fadd_rn(absf, prf);
+    }
+    if (absf < cp.cut_lo || absf > cp.cut_hi) return make_float2(0.0f, 0.0f);
     // --- RCMC (aliased frequency, range walk)
     float fn = bf;
     if (cp.dc < 0.0f) {
@@ -442,8 +504,7 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
         if (fn < fadd_rn(-half, cp.dc)) fn = fadd_rn(fn, prf);
     }
     const float num = fmul_rn(fmul_rn(fmul_rn(a.lambda, a.lambda), fn), fn);
-    const float den = fmul_rn(fmul_rn(8.0f, cp.vr), cp.vr);
-    double dr = static_cast<double>(fdiv_rn(num, den));
+    double dr = static_cast<double>(fdiv_rn(num, cp.den));
     dr *= cp.r0;
     const float shift = static_cast<float>(dr * cp.inv_dr);
     const int walk = static_cast<int>(roundf(shift));
@@ -464,10 +525,7 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
             for (int i = 0; i < kRcmcTaps; ++i) {
                 const float arg = fsub_rn(off, static_cast<float>(i));
                 float sinc = 1.0f;
-                if (arg != 0.0f) {
-                    const float pa = fmul_rn(pi, arg);
-                    sinc = fmul_rn((i & 1) ? -s_off : s_off, rcp_f32(pa));
-                }
+                if (arg != 0.0f) sinc = fast_div((i & 1) ? -s_off : s_off, fmul_rn(pi, arg));
                 const float wgt = fmul_rn(ASARF_LDG(a.win + i), sinc);
                 const float2 d = srow[first + i];
                 si = fma_rn(d.x, wgt, si);
@@ -475,19 +533,12 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
                 nrm = fadd_rn(nrm, wgt);
             }
             if (nrm != 0.0f) {
-                const float inv = rcp_f32(nrm);
+                const float inv = fast_div(1.0f, nrm);
                 out = make_float2(fmul_rn(si, inv), fmul_rn(sq, inv));
             }
         }
     }
-    // --- azimuth matched filter
-    float absf = bf;
-    if (cp.dc < 0.0f) {
-        if (bf > fadd_rn(half, cp.dc)) absf = fsub_rn(absf, prf);
-    } else if (cp.dc > 0.0f) {
-        if (absf < fadd_rn(-half, cp.dc)) absf = fadd_rn(absf, prf);
-    }
-    if (absf < cp.cut_lo || absf > cp.cut_hi) return make_float2(0.0f, 0.0f);
+    // --- matched filter exp(-j pi fc^2 / Ka) * exp(-j 2 pi (dc_off / Ka) f)
     float fc = fsub_rn(bf, cp.dc_off);
     if (fc > half) fc = fsub_rn(fc, prf);
     else if (fc < -half) fc = fadd_rn(fc, prf);
@@ -495,7 +546,7 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
     const float mf_phase = fdiv_rn(fmul_rn(fmul_rn(pi, fc), fc), cp.ka);
     float s1, c1, s2, c2;
     sincosf(mf_phase, &s1, &c1);
-    const float sh_phase = fmul_rn(fmul_rn(fmul_rn(2.0f, pi), fdiv_rn(cp.dc_off, cp.ka)), bf);
+    const float sh_phase = fmul_rn(fmul_rn(fmul_rn(2.0f, pi), cp.dc_off_ka), bf);
     sincosf(sh_phase, &s2, &c2);
     const float2 mf = cmul(make_float2(c1, -s1), make_float2(c2, -s2));
     return cmul(out, mf);

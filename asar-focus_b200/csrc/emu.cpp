@@ -122,8 +122,9 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
     st.dc_step = dc_step;
     st.nblk = nblk;
     st.lines_per_cta = 64;
+    st.vec_ok = (reinterpret_cast<uintptr_t>(d_raw) % 8 == 0) && (raw_line_bytes % 8 == 0) ? 1 : 0;
     st.acc = &g_emu_scratch.acc;
-    backend_raw_stats(st, (range_size + 255) / 256, (azimuth_size + 63) / 64, 256, 256, nullptr);
+    backend_raw_stats(st, (range_size + 1023) / 1024, (azimuth_size + 63) / 64, 256, 1024, nullptr);
     FinalizeArgs fin{};
     fin.acc = &g_emu_scratch.acc;
     fin.state = &g_emu_scratch.state;

@@ -693,7 +693,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     st.nblk = nblk;
     st.lines_per_cta = 64;
     st.acc = p->acc;
-    p->stats_cols = 256;
+    p->stats_cols = 1024;  // 4 columns per thread, 256 threads
     p->stats_gx = (p->nr + p->stats_cols - 1) / p->stats_cols;
     p->stats_gy = (p->na + st.lines_per_cta - 1) / st.lines_per_cta;
 
@@ -774,6 +774,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     d.wt = p->xt2 + p->hl + p->hr;
     d.chunk_rows = 8;
     d.prf = static_cast<float>(s.prf);
+    d.bin_step = d.prf / static_cast<float>(p->az_pad);
+    d.half_prf = d.prf * 0.5f;
     d.lambda = static_cast<float>(s.wavelength);
     d.frac = static_cast<float>(s.az_bw_frac);
     d.slant = s.slant_range_first;
@@ -891,6 +893,7 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     st.raw = d_raw;
     st.swst = d_swst;
     st.min_swst = min_swst;
+    st.vec_ok = (reinterpret_cast<uintptr_t>(d_raw) % 8 == 0) && (p->scene.raw_line_bytes % 8 == 0) ? 1 : 0;
     mark();
     rc = backend_raw_stats(st, p->stats_gx, p->stats_gy, 256, p->stats_cols, stream);
     if (rc) return rc;

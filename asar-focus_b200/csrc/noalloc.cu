@@ -130,8 +130,9 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
     st.dc_step = dc_step;
     st.nblk = nblk;
     st.lines_per_cta = 64;
+    st.vec_ok = (reinterpret_cast<uintptr_t>(d_raw) % 8 == 0) && (raw_line_bytes % 8 == 0) ? 1 : 0;
     st.acc = &scratch->acc;
-    const int cols = 256;
+    const int cols = 1024;
     dim3 grid((range_size + cols - 1) / cols, (azimuth_size + st.lines_per_cta - 1) / st.lines_per_cta);
     k_noalloc_raw_stats<<<grid, 256, 0, s>>>(st, cols);
 

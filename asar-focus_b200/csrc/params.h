@@ -72,6 +72,7 @@ struct RawStatsArgs {
     int min_swst;
     int dc_step, nblk;
     int lines_per_cta;
+    int vec_ok;           // raw base and line stride 8-byte aligned: 4 samples per load
     StatAccum* acc;
 };
 
@@ -111,7 +112,7 @@ struct AzStridedArgs {
 };
 
 struct ColParams {
-    float dc, vr, dc_off, ka, cut_lo, cut_hi;
+    float dc, vr, dc_off, ka, cut_lo, cut_hi, den, dc_off_ka;
     double r0, inv_dr;
 };
 
@@ -126,6 +127,8 @@ struct AzRdArgs {
     int xt, hl, hr, wt;
     int chunk_rows;
     float prf, lambda, frac;
+    float bin_step;       // prf / az_pad (float, as the reference divides)
+    float half_prf;       // prf * 0.5
     double slant, range_spacing;
     float vr_poly[3];
     const FocusState* state;
