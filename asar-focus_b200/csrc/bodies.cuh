@@ -23,6 +23,14 @@ ASARF_HD ASARF_INLINE void atomic_or_u32(unsigned int* p, unsigned int v) {
 #endif
 }
 
+// numpy.blackman(16) in float32, the RCMC tap window (sar/range_doppler_algorithm.cu:46-52):
+// 0.42 - 0.5 cos(2 pi n / 15) + 0.08 cos(4 pi n / 15) rounded to float.
+#define ASARF_BLACKMAN16                                                                                      \
+    {-1.3877787807814457e-17f, 0.016757719218730927f, 0.07707241922616959f, 0.20077013969421387f,             \
+     0.3940124213695526f,      0.6299999952316284f,   0.8492298722267151f,  0.9821574091911316f,              \
+     0.9821574091911316f,      0.8492298722267151f,   0.6299999952316284f,  0.3940124213695526f,              \
+     0.20077013969421387f,     0.07707241922616959f,  0.016757719218730927f, -1.3877787807814457e-17f}
+
 // Device Polyval<N> of the reference (float Horner; nvcc contracts r*x + e into one fma).
 template <int N>
 ASARF_HD ASARF_INLINE float polyval_f32(const float (&p)[N], float x) {
@@ -117,64 +125,87 @@ ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by,
         int pi[4] = {0, 0, 0, 0}, pq[4] = {0, 0, 0, 0};
         bool pf[4] = {false, false, false, false};
         if (xin) {
-            for (int y = ys; y < y1; ++y) {
-                const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
-                const int i0 = xb - off;
-                const uint8_t* rowp = a.raw + static_cast<long long>(y) * a.line_bytes;
-                int iv[4], qv[4];
-                bool f[4];
-                if (a.vec_ok && i0 >= 0 && i0 + 4 <= a.spl && xb + 4 <= a.nr) {
-                    const uint2 w = *reinterpret_cast<const uint2*>(rowp + 2ll * i0);
-                    iv[0] = w.x & 0xff;
-                    qv[0] = (w.x >> 8) & 0xff;
-                    iv[1] = (w.x >> 16) & 0xff;
-                    qv[1] = w.x >> 24;
-                    iv[2] = w.y & 0xff;
-                    qv[2] = (w.y >> 8) & 0xff;
-                    iv[3] = (w.y >> 16) & 0xff;
-                    qv[3] = w.y >> 24;
-                    f[0] = f[1] = f[2] = f[3] = true;
-                } else {
-                    for (int k = 0; k < 4; ++k) {
-                        const int i = i0 + k;
-                        f[k] = (xb + k < a.nr) && (i >= 0) && (i < a.spl);
-                        iv[k] = qv[k] = 0;
-                        if (f[k]) {
-                            const uint16_t w = *reinterpret_cast<const uint16_t*>(rowp + 2ll * i);
-                            iv[k] = w & 0xff;
-                            qv[k] = w >> 8;
-                        }
-                    }
-                }
-                if (y >= y0) {
+            // lines in groups of 4: the group's loads are issued before any is consumed
+            for (int yg = ys; yg < y1; yg += 4) {
+                uint2 wv[4];
+                int i0v[4];
+                bool vec[4];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (f[k]) {
-                            cnt += 1;
-                            si += iv[k];
-                            sq += qv[k];
-                            sii += iv[k] * iv[k];
-                            sqq += qv[k] * qv[k];
-                            siq += iv[k] * qv[k];
-                        }
-                        if (y > 0 && f[k] && pf[k]) {
-                            l[k][0] += 1;
-                            l[k][1] += pi[k];
-                            l[k][2] += pq[k];
-                            l[k][3] += iv[k];
-                            l[k][4] += qv[k];
-                            l[k][5] += pi[k] * iv[k];
-                            l[k][6] += pq[k] * qv[k];
-                            l[k][7] += pi[k] * qv[k];
-                            l[k][8] += pq[k] * iv[k];
-                        }
+                for (int u = 0; u < 4; ++u) {
+                    const int y = yg + u;
+                    vec[u] = false;
+                    i0v[u] = 0;
+                    wv[u] = make_uint2(0u, 0u);
+                    if (y < y1) {
+                        const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
+                        i0v[u] = xb - off;
+                        vec[u] = a.vec_ok && i0v[u] >= 0 && i0v[u] + 4 <= a.spl && xb + 4 <= a.nr;
+                        if (vec[u])
+                            wv[u] = *reinterpret_cast<const uint2*>(a.raw + static_cast<long long>(y) * a.line_bytes +
+                                                                    2ll * i0v[u]);
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    pi[k] = iv[k];
-                    pq[k] = qv[k];
-                    pf[k] = f[k];
+                for (int u = 0; u < 4; ++u) {
+                    const int y = yg + u;
+                    if (y >= y1) break;
+                    const int i0 = i0v[u];
+                    int iv[4], qv[4];
+                    bool f[4];
+                    if (vec[u]) {
+                        const uint2 w = wv[u];
+                        iv[0] = w.x & 0xff;
+                        qv[0] = (w.x >> 8) & 0xff;
+                        iv[1] = (w.x >> 16) & 0xff;
+                        qv[1] = w.x >> 24;
+                        iv[2] = w.y & 0xff;
+                        qv[2] = (w.y >> 8) & 0xff;
+                        iv[3] = (w.y >> 16) & 0xff;
+                        qv[3] = w.y >> 24;
+                        f[0] = f[1] = f[2] = f[3] = true;
+                    } else {
+                        const uint8_t* rowp = a.raw + static_cast<long long>(y) * a.line_bytes;
+                        for (int k = 0; k < 4; ++k) {
+                            const int i = i0 + k;
+                            f[k] = (xb + k < a.nr) && (i >= 0) && (i < a.spl);
+                            iv[k] = qv[k] = 0;
+                            if (f[k]) {
+                                const uint16_t w = *reinterpret_cast<const uint16_t*>(rowp + 2ll * i);
+                                iv[k] = w & 0xff;
+                                qv[k] = w >> 8;
+                            }
+                        }
+                    }
+                    if (y >= y0) {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (f[k]) {
+                                cnt += 1;
+                                si += iv[k];
+                                sq += qv[k];
+                                sii += iv[k] * iv[k];
+                                sqq += qv[k] * qv[k];
+                                siq += iv[k] * qv[k];
+                            }
+                            if (y > 0 && f[k] && pf[k]) {
+                                l[k][0] += 1;
+                                l[k][1] += pi[k];
+                                l[k][2] += pq[k];
+                                l[k][3] += iv[k];
+                                l[k][4] += qv[k];
+                                l[k][5] += pi[k] * iv[k];
+                                l[k][6] += pq[k] * qv[k];
+                                l[k][7] += pi[k] * qv[k];
+                                l[k][8] += pq[k] * iv[k];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        pi[k] = iv[k];
+                        pq[k] = qv[k];
+                        pf[k] = f[k];
+                    }
                 }
             }
         }
@@ -520,13 +551,14 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
             // sin(pi (off - i)) = (-1)^i sin(pi off): one sinpi per output instead of one sinf per tap;
             // the denominators pi (off - i) are rounded exactly as the reference rounds them
             const float s_off = sinpi_f32(off);
+            constexpr float kWin[kRcmcTaps] = ASARF_BLACKMAN16;
             float si = 0.0f, sq = 0.0f, nrm = 0.0f;
 #pragma unroll
             for (int i = 0; i < kRcmcTaps; ++i) {
                 const float arg = fsub_rn(off, static_cast<float>(i));
-                float sinc = 1.0f;
-                if (arg != 0.0f) sinc = fast_div((i & 1) ? -s_off : s_off, fmul_rn(pi, arg));
-                const float wgt = fmul_rn(ASARF_LDG(a.win + i), sinc);
+                const float q = fast_div((i & 1) ? -s_off : s_off, fmul_rn(pi, arg));
+                const float sinc = (arg != 0.0f) ? q : 1.0f;
+                const float wgt = fmul_rn(kWin[i], sinc);
                 const float2 d = srow[first + i];
                 si = fma_rn(d.x, wgt, si);
                 sq = fma_rn(d.y, wgt, sq);
@@ -558,6 +590,7 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     const int n2 = a.n2, wt = a.wt;
     const FastDiv dwt = make_fastdiv(static_cast<unsigned int>(wt));
     const FastDiv dxt = make_fastdiv(static_cast<unsigned int>(a.xt));
+    (void)dxt;
     if (!preloaded) {
         for (int t = tid; t < n2 * wt; t += nthr) {
             const int r = static_cast<int>(fdiv_u(t, dwt)), c = t - r * wt;
@@ -570,27 +603,39 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     for (int c = tid; c < a.xt; c += nthr) cps[c] = az_col_params(a, x0 + c);
     ASARF_SYNC();
     fft_forward(a.plan2, s, wt, wt, tid, nthr);
-    // RCMC + matched filter, chunk_rows rows at a time through tmp (in-place safe)
-    for (int r0 = 0; r0 < n2; r0 += a.chunk_rows) {
-        const int rn = (r0 + a.chunk_rows < n2) ? a.chunk_rows : n2 - r0;
-        for (int t = tid; t < rn * a.xt; t += nthr) {
-            const int rr = static_cast<int>(fdiv_u(t, dxt)), c = t - rr * a.xt;
-            const int p = r0 + rr;
-            const int x = x0 + c;
-            float2 v = make_float2(0.0f, 0.0f);
-            if (x < a.nk) {
-                const int f = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
-                v = rcmc_mf_sample(a, cps[c], x, f, s + p * wt, a.hl + c, err_flag);
-            }
-            tmp[t] = v;
+    // RCMC + matched filter.  Every output (row p, column c) reads taps of row p only, so a
+    // row is computed into registers by one warp (lane = column, xt <= 64), the warp
+    // synchronises, and writes it back in place: no block-wide barrier per row.
+#if defined(__CUDA_ARCH__)
+    {
+        const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+        for (int p = warp; p < n2; p += nwarps) {
+            const int f = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
+            const float2* srow = s + p * wt;
+            float2 v0 = make_float2(0.0f, 0.0f), v1 = make_float2(0.0f, 0.0f);
+            const int c0 = lane, c1 = lane + 32;
+            if (c0 < a.xt && x0 + c0 < a.nk) v0 = rcmc_mf_sample(a, cps[c0], x0 + c0, f, srow, a.hl + c0, err_flag);
+            if (c1 < a.xt && x0 + c1 < a.nk) v1 = rcmc_mf_sample(a, cps[c1], x0 + c1, f, srow, a.hl + c1, err_flag);
+            __syncwarp();
+            if (c0 < a.xt) s[p * wt + a.hl + c0] = v0;
+            if (c1 < a.xt) s[p * wt + a.hl + c1] = v1;
+            __syncwarp();
         }
-        ASARF_SYNC();
-        for (int t = tid; t < rn * a.xt; t += nthr) {
-            const int rr = static_cast<int>(fdiv_u(t, dxt)), c = t - rr * a.xt;
-            s[(r0 + rr) * wt + a.hl + c] = tmp[t];
-        }
-        ASARF_SYNC();
     }
+    ASARF_SYNC();
+#else
+    {
+        float2 rowbuf[64];
+        for (int p = 0; p < n2; ++p) {
+            const int f = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
+            for (int c = 0; c < a.xt; ++c)
+                rowbuf[c] = (x0 + c < a.nk) ? rcmc_mf_sample(a, cps[c], x0 + c, f, s + p * wt, a.hl + c, err_flag)
+                                            : make_float2(0.0f, 0.0f);
+            for (int c = 0; c < a.xt; ++c) s[p * wt + a.hl + c] = rowbuf[c];
+        }
+        (void)tmp;
+    }
+#endif
     fft_inverse(a.plan2, s + a.hl, a.xt, wt, tid, nthr);
     for (int t = tid; t < n2 * a.xt; t += nthr) {
         const int r = static_cast<int>(fdiv_u(t, dxt)), c = t - r * a.xt;
@@ -621,15 +666,17 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
     const int c0 = e0 > s0 ? e0 - s0 : 0;
     const int c1 = e1 > s1 ? e1 - s1 : 0;
     const float2* base = a.slc + static_cast<long long>(st.first_line) * a.pitch + a.col0;
+    const int r_lo = s0 < s1 ? s0 : s1;
+    const int r_hi = e0 > e1 ? e0 : e1;
+    // each input row is read once and added to whichever box mean(s) contain it, in row
+    // order, so both sums accumulate exactly as the reference's two loops do
     for (int c = tid; c < a.nx; c += nthr) {
         float sum0 = 0.0f, sum1 = 0.0f;
-        for (int r = s0; r < e0; ++r) {
+        for (int r = r_lo; r < r_hi; ++r) {
             const float2 v = base[static_cast<long long>(r) * a.pitch + c];
-            sum0 = fadd_rn(sum0, fma_rn(v.x, v.x, fmul_rn(v.y, v.y)));
-        }
-        for (int r = s1; r < e1; ++r) {
-            const float2 v = base[static_cast<long long>(r) * a.pitch + c];
-            sum1 = fadd_rn(sum1, fma_rn(v.x, v.x, fmul_rn(v.y, v.y)));
+            const float p2 = fma_rn(v.x, v.x, fmul_rn(v.y, v.y));
+            if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
+            if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
         }
         if (c0) sum0 = fdiv_rn(sum0, static_cast<float>(c0));
         if (c1) sum1 = fdiv_rn(sum1, static_cast<float>(c1));

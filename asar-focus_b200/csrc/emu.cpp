@@ -43,7 +43,7 @@ int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, Launch
     std::vector<float2> buf(sh.smem / sizeof(float2) + 16);
     float2* s = buf.data();
     float2* tmp = s + a.n2 * a.wt;
-    ColParams* cps = reinterpret_cast<ColParams*>(tmp + a.chunk_rows * a.xt);
+    ColParams* cps = reinterpret_cast<ColParams*>(tmp);
     for (int b = 0; b < nblocks; ++b)
         for (int t = 0; t < tiles; ++t) az_rd_body(a, t, b, 0, 1, s, tmp, cps, err, false);
     return ASARF_OK;

@@ -564,11 +564,11 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         const double walk = s.wavelength * s.wavelength * f * f * rmax / (8 * vr_min * vr_min) / s.range_spacing;
         p->hl = kRcmcTaps / 2;
         p->hr = kRcmcTaps / 2 + static_cast<int>(std::ceil(walk)) + 2;
-        if ((32 + p->hl + p->hr) & 1) ++p->hr;  // even tile width: TMA rows are whole 16-byte units
+        if ((64 + p->hl + p->hr) & 1) ++p->hr;  // even tile width: TMA rows are whole 16-byte units
     }
     p->pitch = (p->nk + 31) / 32 * 32;
     p->xt1 = (p->n1 * 32 * 8 <= 160 * 1024) ? 32 : 16;
-    p->xt2 = 32;
+    p->xt2 = 64;
 
     // chirp matched filter in the forward transform's output order, scaled by 1/L
     std::vector<std::complex<float>> chirp;
@@ -697,6 +697,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     p->stats_gx = (p->nr + p->stats_cols - 1) / p->stats_cols;
     p->stats_gy = (p->na + st.lines_per_cta - 1) / st.lines_per_cta;
 
+
     FinalizeArgs& fin = p->a_fin;
     fin.acc = p->acc;
     fin.state = p->state;
@@ -772,7 +773,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     d.hl = p->hl;
     d.hr = p->hr;
     d.wt = p->xt2 + p->hl + p->hr;
-    d.chunk_rows = 8;
+    d.chunk_rows = 0;
     d.prf = static_cast<float>(s.prf);
     d.bin_step = d.prf / static_cast<float>(p->az_pad);
     d.half_prf = d.prf * 0.5f;
@@ -784,8 +785,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     d.state = p->state;
     d.win = win;
     p->tiles2 = (p->nk + p->xt2 - 1) / p->xt2;
-    p->sh_rd = {256, sizeof(float2) * (static_cast<size_t>(p->n2) * d.wt + static_cast<size_t>(d.chunk_rows) * d.xt) +
-                         sizeof(ColParams) * d.xt + 16};
+    p->sh_rd = {512, sizeof(float2) * static_cast<size_t>(p->n2) * d.wt + sizeof(ColParams) * d.xt + 16};
 
     TailArgs& t = p->a_tail;
     t.slc = p->bufB;

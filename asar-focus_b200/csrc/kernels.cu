@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
     const int wt = a.wt;
     float2* s = reinterpret_cast<float2*>(smem_rd_raw);
     float2* tmp = s + a.n2 * wt;
-    ColParams* cps = reinterpret_cast<ColParams*>(tmp + a.chunk_rows * a.xt);
+    ColParams* cps = reinterpret_cast<ColParams*>(tmp);
     __shared__ uint64_t bar;
     if (a.use_tma) {
         if (threadIdx.x == 0) {
