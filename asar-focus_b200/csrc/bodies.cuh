@@ -10,6 +10,7 @@
 #include <cstdint>
 
 #include "fft.cuh"
+#include "fft_ct.cuh"
 #include "hd.cuh"
 #include "params.h"
 
@@ -403,6 +404,53 @@ ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y
     fft_inverse(a.plan, s, 1, 1, tid, nthr);
     float2* orow = a.out + static_cast<long long>(y) * a.out_pitch;
     for (int l = tid; l < a.nk; l += nthr) orow[l] = s[l];
+}
+
+// Same transform with a compile-time schedule (lengths in kCtLengths): all loops unrolled,
+// all index arithmetic constant.
+template <int L>
+ASARF_HD ASARF_INLINE void range_compress_ct_body(const RangeCompressArgs& a, int y, int tid, float2* s,
+                                                  const uint8_t* raw_line) {
+    constexpr int NTHR = CtSchedule<L>::nthr;
+    constexpr int PER = (L + NTHR - 1) / NTHR;
+    const FocusState& st = *a.state;
+    const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
+    const uint8_t* row = raw_line ? raw_line : a.raw + static_cast<long long>(y) * a.line_bytes;
+    const float2* __restrict__ tw = a.plan.tw;
+    ct_phase<NTHR>(
+        [&](int t) {
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int l = t + k * NTHR;
+                if (L % NTHR != 0 && l >= L) break;
+                float2 z = make_float2(0.0f, 0.0f);
+                const int i = l - off;
+                if (l < a.nr && i >= 0 && i < a.spl) {
+                    const uint16_t wv = *reinterpret_cast<const uint16_t*>(row + 2ll * i);
+                    z = correct_sample(wv & 0xff, wv >> 8, st);
+                }
+                s[l] = z;
+            }
+        },
+        tid);
+    ct_fft_forward<L>(s, tw, tid);
+    ct_phase<NTHR>(
+        [&](int t) {
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int l = t + k * NTHR;
+                if (L % NTHR != 0 && l >= L) break;
+                s[l] = cmul(s[l], ASARF_LDG(a.mf + l));
+            }
+        },
+        tid);
+    ct_fft_inverse<L>(s, tw, tid);
+    float2* orow = a.out + static_cast<long long>(y) * a.out_pitch;
+    ct_phase<NTHR>(
+        [&](int t) {
+            for (int l = t; l < a.nk; l += NTHR) orow[l] = s[l];
+        },
+        tid);
 }
 
 // ----------------------------------------------------------------------------- azimuth strided pass

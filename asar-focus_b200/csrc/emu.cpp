@@ -26,8 +26,24 @@ int backend_finalize(const FinalizeArgs& a, void*) {
     return ASARF_OK;
 }
 
+template <int L>
+static void emu_rc_ct(const RangeCompressArgs& a, int lines, float2* s) {
+    for (int y = 0; y < lines; ++y) range_compress_ct_body<L>(a, y, 0, s, nullptr);
+}
+
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void*) {
     std::vector<float2> s(sh.smem / sizeof(float2) + 1);
+    switch (a.plan.n) {
+        case 768: emu_rc_ct<768>(a, lines, s.data()); return ASARF_OK;
+        case 1024: emu_rc_ct<1024>(a, lines, s.data()); return ASARF_OK;
+        case 1536: emu_rc_ct<1536>(a, lines, s.data()); return ASARF_OK;
+        case 2048: emu_rc_ct<2048>(a, lines, s.data()); return ASARF_OK;
+        case 3072: emu_rc_ct<3072>(a, lines, s.data()); return ASARF_OK;
+        case 4096: emu_rc_ct<4096>(a, lines, s.data()); return ASARF_OK;
+        case 6144: emu_rc_ct<6144>(a, lines, s.data()); return ASARF_OK;
+        case 8192: emu_rc_ct<8192>(a, lines, s.data()); return ASARF_OK;
+        default: break;
+    }
     for (int y = 0; y < lines; ++y) range_compress_body(a, y, 0, 1, s.data(), nullptr);
     return ASARF_OK;
 }

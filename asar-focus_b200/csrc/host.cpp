@@ -329,6 +329,9 @@ static bool build_fft(int n, HostFft& h) {
 }
 
 static int choose_rc_len(int nr) {
+    // a compile-time-scheduled length when one is close above (within 1.5x)
+    for (int L : kCtLengths)
+        if (L >= nr && 2 * L <= 3 * nr) return L;
     int best = -1;
     double bc = 1e30;
     for (int n = nr; n <= 2 * nr + 64; ++n) {

@@ -49,6 +49,30 @@ __global__ void __launch_bounds__(512) k_range_compress(RangeCompressArgs a) {
     range_compress_body(a, blockIdx.x, threadIdx.x, blockDim.x, s, line);
 }
 
+// Compile-time-scheduled variant (L in kCtLengths).
+template <int L>
+__global__ void __launch_bounds__(CtSchedule<L>::nthr, 2) k_range_compress_ct(RangeCompressArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_rcc_raw[];
+    float2* s = reinterpret_cast<float2*>(smem_rcc_raw);
+    __shared__ uint64_t bar;
+    const uint8_t* line = nullptr;
+    if (a.bulk_bytes > 0) {
+        uint8_t* buf = smem_rcc_raw + a.raw_smem_offset;
+        const uint8_t* src = a.raw + static_cast<long long>(blockIdx.x) * a.line_bytes;
+        const int total = 2 * a.spl;
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_expect_tx(&bar, static_cast<uint32_t>(a.bulk_bytes));
+            bulk_load(buf, src, static_cast<uint32_t>(a.bulk_bytes), &bar);
+        }
+        for (int i = a.bulk_bytes + threadIdx.x; i < total; i += blockDim.x) buf[i] = src[i];
+        __syncthreads();
+        mbar_wait(&bar, 0, &const_cast<FocusState*>(a.state)->errors);
+        line = buf;
+    }
+    range_compress_ct_body<L>(a, blockIdx.x, threadIdx.x, s, line);
+}
+
 // Strided azimuth pass: the [n1][xt] tile (rows r*n2 + b) arrives by 3-D TMA boxes.
 __global__ void __launch_bounds__(512) k_az_strided(AzStridedArgs a, const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(1024) unsigned char smem_as_raw[];
@@ -124,7 +148,26 @@ int backend_finalize(const FinalizeArgs& a, void* stream) {
     return check_launch("finalize");
 }
 
+template <int L>
+static int launch_rc_ct(const RangeCompressArgs& a, int lines, size_t smem, void* stream) {
+    int rc = ensure_smem(k_range_compress_ct<L>, smem, "range_compress");
+    if (rc) return rc;
+    k_range_compress_ct<L><<<lines, CtSchedule<L>::nthr, smem, S(stream)>>>(a);
+    return check_launch("range_compress");
+}
+
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void* stream) {
+    switch (a.plan.n) {
+        case 768: return launch_rc_ct<768>(a, lines, sh.smem, stream);
+        case 1024: return launch_rc_ct<1024>(a, lines, sh.smem, stream);
+        case 1536: return launch_rc_ct<1536>(a, lines, sh.smem, stream);
+        case 2048: return launch_rc_ct<2048>(a, lines, sh.smem, stream);
+        case 3072: return launch_rc_ct<3072>(a, lines, sh.smem, stream);
+        case 4096: return launch_rc_ct<4096>(a, lines, sh.smem, stream);
+        case 6144: return launch_rc_ct<6144>(a, lines, sh.smem, stream);
+        case 8192: return launch_rc_ct<8192>(a, lines, sh.smem, stream);
+        default: break;
+    }
     int rc = ensure_smem(k_range_compress, sh.smem, "range_compress");
     if (rc) return rc;
     k_range_compress<<<lines, sh.threads, sh.smem, S(stream)>>>(a);
