@@ -64,6 +64,17 @@ class RawStats(C.Structure):
     ]
 
 
+class IqResults(C.Structure):
+    _fields_ = [("dc_i", C.c_double), ("dc_q", C.c_double), ("iq_gain", C.c_double), ("phase_error", C.c_double),
+                ("stddev_i", C.c_double), ("stddev_q", C.c_double)]
+
+
+class RdaParams(C.Structure):
+    _fields_ = [("prf", C.c_double), ("wavelength", C.c_double), ("range_spacing", C.c_double),
+                ("slant_range_first", C.c_double), ("az_bw_frac", C.c_double), ("vr_poly", C.c_double * 3),
+                ("dc_poly", C.c_double * 3)]
+
+
 class AsarfError(RuntimeError):
     pass
 
@@ -95,6 +106,26 @@ _SIGS = {
     "asarf_raw_statistics_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                                C.c_int32, C.c_int64, C.c_int32, C.c_double, C.c_void_p,
                                                C.c_void_p]),
+    # per-stage entry points
+    "asarf_convert_ers_samples": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
+                                            C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
+    "asarf_raw_data_correction": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+                                            C.POINTER(IqResults), C.c_void_p]),
+    "asarf_zero_nans": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "asarf_doppler_centroid": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                         C.POINTER(C.c_double * 3), C.c_void_p]),
+    "asarf_range_compression": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float),
+                                          C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.c_void_p]),
+    "asarf_range_doppler": (C.c_int, [C.POINTER(RdaParams), C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_int32, C.c_void_p]),
+    "asarf_azimuth_multilook": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p,
+                                          C.POINTER(C.c_int32), C.c_void_p]),
+    "asarf_range_spreading_loss": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                             C.c_void_p]),
+    "asarf_srgr": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double * 5), C.c_double, C.c_int32,
+                             C.c_void_p, C.c_void_p]),
+    "asarf_srgr_index": (C.c_int, [C.POINTER(C.c_double * 5), C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]),
 }
 
 _cache: dict[str, C.CDLL] = {}

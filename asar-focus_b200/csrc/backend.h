@@ -22,6 +22,17 @@ int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, L
                   void* stream);
 int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err, void* stream);
 
+// per-stage kernels
+int backend_decode(const DecodeArgs& a, long long n, void* stream);
+int backend_img_moments(const ImgMomentsArgs& a, int blocks, void* stream);
+int backend_iq_apply(const IqApplyArgs& a, long long n, void* stream);
+int backend_zero_nans(float2* img, long long n, void* stream);
+int backend_accc(const AcccArgs& a, int blocks, void* stream);
+int backend_rc_rows(const RcRowsArgs& a, int rows, LaunchShape sh, void* stream);
+int backend_multilook(const MultilookArgs& a, void* stream);
+int backend_rsl(const RslArgs& a, long long n, void* stream);
+int backend_srgr(const SrgrArgs& a, long long n, void* stream);
+
 void* mem_alloc(size_t bytes);
 void mem_free(void* p);
 int mem_h2d(void* dst, const void* src, size_t n, void* stream);

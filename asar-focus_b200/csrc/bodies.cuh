@@ -749,4 +749,178 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
     }
 }
 
+// ============================================================================= per-stage bodies
+
+// ConvertErsImSamplesToComplexKernel (envisat_format/src/envisat_format_kernels.cu:116-134)
+// after the NaN pre-fill of ConvertRawSampleSetsToComplex (main_flow.cc:537-540): one item
+// per (line, range sample).
+ASARF_HD ASARF_INLINE void decode_item(const DecodeArgs& a, long long idx) {
+    const int y = static_cast<int>(idx / a.nr);
+    const int x = static_cast<int>(idx - static_cast<long long>(y) * a.nr);
+    const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
+    const int i = x - off;
+    float2 v = make_float2(qnan_f(), qnan_f());
+    if (i >= 0 && i < a.spl) {
+        const uint8_t* p = a.raw + static_cast<long long>(y) * a.line_bytes + 2ll * i;
+        v = make_float2(static_cast<float>(p[0]), static_cast<float>(p[1]));
+    }
+    a.img[static_cast<long long>(y) * a.stride + x] = v;
+}
+
+ASARF_HD ASARF_INLINE bool is_nan_f(float v) { return v != v; }
+
+// Moment partials for RawDataCorrection / CalcMean / CalcStdDev
+// (sar/iq_correction.cu:40-138, cuda_util/device_padded_image.cu:156-257): block `blk` sums
+// rows [blk*rpb, ...) in double, NaN samples skipped; deterministic in-block tree.
+ASARF_HD ASARF_INLINE void img_moments_body(const ImgMomentsArgs& a, int blk, int tid, int nthr, double* red) {
+    double acc[12];
+    for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+    const int y0 = blk * a.rows_per_block;
+    const int y1 = (y0 + a.rows_per_block < a.y_size) ? y0 + a.rows_per_block : a.y_size;
+    for (int y = y0; y < y1; ++y) {
+        const float2* row = a.img + static_cast<long long>(y) * a.x_stride;
+        for (int x = tid; x < a.x_stride; x += nthr) {
+            const float2 v = row[x];
+            if (is_nan_f(v.x) || is_nan_f(v.y)) continue;
+            const int o = x < a.x_size ? 0 : 6;
+            if (a.centered) {
+                if (o) continue;
+                const float di = fsub_rn(v.x, a.mean_i), dq = fsub_rn(v.y, a.mean_q);
+                acc[3] += static_cast<double>(fmul_rn(di, di));
+                acc[4] += static_cast<double>(fmul_rn(dq, dq));
+                acc[0] += 1.0;
+                continue;
+            }
+            const double i = v.x, q = v.y;
+            acc[o + 0] += 1.0;
+            acc[o + 1] += i;
+            acc[o + 2] += q;
+            acc[o + 3] += i * i;
+            acc[o + 4] += q * q;
+            acc[o + 5] += i * q;
+        }
+    }
+    for (int k = 0; k < 12; ++k) red[k * nthr + tid] = acc[k];
+    ASARF_SYNC();
+#if defined(__CUDA_ARCH__)
+    for (int w = nthr / 2; w > 0; w >>= 1) {
+        if (tid < w)
+            for (int k = 0; k < 12; ++k) red[k * nthr + tid] += red[k * nthr + tid + w];
+        ASARF_SYNC();
+    }
+    if (tid == 0)
+        for (int k = 0; k < 12; ++k) a.partial[blk * 12 + k] = red[k * nthr];
+#else
+    for (int k = 0; k < 12; ++k) a.partial[blk * 12 + k] = red[k * nthr];
+#endif
+}
+
+// CorrectDCBias + ApplyGainCorrection + ApplyPhaseCorrection (sar/iq_correction.cu:140-178)
+// over x < XStride, y < YSize; NaN stays NaN.
+ASARF_HD ASARF_INLINE void iq_apply_item(const IqApplyArgs& a, long long idx) {
+    float2 v = a.img[idx];
+    const float i1 = fsub_rn(v.x, a.dc_i);
+    const float q1 = fsub_rn(v.y, a.dc_q);
+    const float i2 = fdiv_rn(i1, a.gain);
+    const float q2 = fdiv_rn(fma_rn(-i2, a.sin_c, q1), a.cos_c);
+    a.img[idx] = make_float2(i2, q2);
+}
+
+// PhaseDifference partials of CalculateDopplerCentroid (sar/fractional_doppler_centroid.cu:33-69):
+// per block of rows and per column x (columns up to nblk*step, which may reach into the
+// padding as the reference's last block does), the FP64 sum over pairs (y-1, y), y >= 1,
+// of conj(z[y-1]) z[y]; the host adds columns into range blocks in a fixed order.
+ASARF_HD ASARF_INLINE void accc_body(const AcccArgs& a, int blk, int tid, int nthr) {
+    const int y0 = blk * a.rows_per_block;
+    const int y1 = (y0 + a.rows_per_block < a.y_size) ? y0 + a.rows_per_block : a.y_size;
+    const int xend = a.nblk * a.step < a.x_stride ? a.nblk * a.step : a.x_stride;
+    for (int x = tid; x < xend; x += nthr) {
+        double re = 0.0, im = 0.0;
+        for (int y = (y0 > 1 ? y0 : 1); y < y1; ++y) {
+            const float2 p = a.img[static_cast<long long>(y - 1) * a.x_stride + x];
+            const float2 c = a.img[static_cast<long long>(y) * a.x_stride + x];
+            re += static_cast<double>(p.x) * c.x + static_cast<double>(p.y) * c.y;
+            im += static_cast<double>(p.x) * c.y - static_cast<double>(p.y) * c.x;
+        }
+        a.partial[(static_cast<long long>(blk) * xend + x) * 2] = re;
+        a.partial[(static_cast<long long>(blk) * xend + x) * 2 + 1] = im;
+    }
+}
+
+// RangeCompression on complex rows in place (sar/range_compression.cu:57-111): inputs
+// x < nr, outputs x < nk scaled, [nk, x_zero_end) zeroed (FinishRangeCompression).
+ASARF_HD ASARF_INLINE void rc_rows_body(const RcRowsArgs& a, int y, int tid, int nthr, float2* s) {
+    const int L = a.plan.n;
+    float2* row = a.img + static_cast<long long>(y) * a.stride;
+    for (int l = tid; l < L; l += nthr) s[l] = l < a.nr ? row[l] : make_float2(0.0f, 0.0f);
+    ASARF_SYNC();
+    fft_forward(a.plan, s, 1, 1, tid, nthr);
+    for (int l = tid; l < L; l += nthr) s[l] = cmul(s[l], ASARF_LDG(a.mf + l));
+    ASARF_SYNC();
+    fft_inverse(a.plan, s, 1, 1, tid, nthr);
+    for (int l = tid; l < a.x_zero_end; l += nthr) row[l] = l < a.nk ? s[l] : make_float2(0.0f, 0.0f);
+}
+
+// TimeDomainAzimuthLook (sar/az_multilook.cu:25-80): one output line per block.
+ASARF_HD ASARF_INLINE void multilook_row_body(const MultilookArgs& a, int y, int tid, int nthr) {
+    const float in_idx = fmul_rn(static_cast<float>(y), a.ratio);
+    const float mu = fsub_rn(in_idx, static_cast<float>(static_cast<int>(in_idx)));
+    int s0 = static_cast<int>(fsub_rn(in_idx, 2.0f)), e0 = static_cast<int>(fadd_rn(in_idx, 2.0f));
+    int s1 = static_cast<int>(fsub_rn(in_idx, 1.0f)), e1 = static_cast<int>(fadd_rn(in_idx, 3.0f));
+    s0 = s0 > 0 ? s0 : 0;
+    s1 = s1 > 0 ? s1 : 0;
+    e0 = e0 < a.in_y ? e0 : a.in_y;
+    e1 = e1 < a.in_y ? e1 : a.in_y;
+    const int c0 = e0 > s0 ? e0 - s0 : 0;
+    const int c1 = e1 > s1 ? e1 - s1 : 0;
+    const int r_lo = s0 < s1 ? s0 : s1;
+    const int r_hi = e0 > e1 ? e0 : e1;
+    for (int c = tid; c < a.x_size; c += nthr) {
+        float sum0 = 0.0f, sum1 = 0.0f;
+        for (int r = r_lo; r < r_hi; ++r) {
+            const float2 v = a.slc[static_cast<long long>(r) * a.x_size + c];
+            const float p2 = fma_rn(v.x, v.x, fmul_rn(v.y, v.y));
+            if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
+            if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
+        }
+        if (c0) sum0 = fdiv_rn(sum0, static_cast<float>(c0));
+        if (c1) sum1 = fdiv_rn(sum1, static_cast<float>(c1));
+        float val = 0.0f;
+        if (c0 && c1) val = fma_rn(fsub_rn(sum1, sum0), mu, sum0);
+        a.out[static_cast<long long>(y) * a.x_size + c] = val;
+    }
+}
+
+// CorrectionKernel of RangeSpreadingLossCorrection (sar/range_spreading_loss.cu:29-52).
+ASARF_HD ASARF_INLINE void rsl_item(const RslArgs& a, long long idx) {
+    const int x = static_cast<int>(idx % a.range_size);
+    const double r = a.slant_first + x * a.range_spacing;
+    const double ratio = a.ref_range / r;
+    const float g = static_cast<float>(1.0 / sqrt(pow(ratio, 3.0)));
+    a.img[idx] = fmul_rn(a.img[idx], g);
+}
+
+// SrGrInterpolation (sar/srgr.cu:49-71) with the float Horner / IEEE divide / truncation index.
+ASARF_HD ASARF_INLINE void srgr_item(const SrgrArgs& a, long long idx) {
+    const int y = static_cast<int>(idx / a.out_x);
+    const int xg = static_cast<int>(idx - static_cast<long long>(y) * a.out_x);
+    const float gd = fmul_rn(static_cast<float>(xg), a.ground_spacing);
+    const float rd = polyval_f32(a.grsr, gd);
+    const float ridx = fdiv_rn(rd, a.range_spacing);
+    int i0 = static_cast<int>(ridx);
+    const float dx = fsub_rn(ridx, static_cast<float>(i0));
+    if (a.start && y == 0) {
+        a.start[xg] = i0;
+        a.frac[xg] = dx;
+    }
+    if (!a.in) return;
+    if (i0 < 0 || i0 + 1 >= a.in_x) {
+        if (a.err) atomic_or_u32(a.err, kErrSrgrIndex);
+        i0 = i0 < 0 ? 0 : a.in_x - 2;
+    }
+    const float* row = a.in + static_cast<long long>(y) * a.in_x;
+    const float v0 = row[i0], v1 = row[i0 + 1];
+    a.out[idx] = fma_rn(dx, fsub_rn(v1, v0), v0);
+}
+
 }  // namespace asarf

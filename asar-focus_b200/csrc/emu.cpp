@@ -71,6 +71,48 @@ int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err,
     return ASARF_OK;
 }
 
+int backend_decode(const DecodeArgs& a, long long n, void*) {
+    for (long long i = 0; i < n; ++i) decode_item(a, i);
+    return ASARF_OK;
+}
+int backend_img_moments(const ImgMomentsArgs& a, int blocks, void*) {
+    std::vector<double> red(12);
+    for (int b = 0; b < blocks; ++b) img_moments_body(a, b, 0, 1, red.data());
+    return ASARF_OK;
+}
+int backend_iq_apply(const IqApplyArgs& a, long long n, void*) {
+    for (long long i = 0; i < n; ++i) iq_apply_item(a, i);
+    return ASARF_OK;
+}
+int backend_zero_nans(float2* img, long long n, void*) {
+    for (long long i = 0; i < n; ++i) {
+        if (is_nan_f(img[i].x)) img[i].x = 0.0f;
+        if (is_nan_f(img[i].y)) img[i].y = 0.0f;
+    }
+    return ASARF_OK;
+}
+int backend_accc(const AcccArgs& a, int blocks, void*) {
+    for (int b = 0; b < blocks; ++b) accc_body(a, b, 0, 1);
+    return ASARF_OK;
+}
+int backend_rc_rows(const RcRowsArgs& a, int rows, LaunchShape sh, void*) {
+    std::vector<float2> s(sh.smem / sizeof(float2) + 1);
+    for (int y = 0; y < rows; ++y) rc_rows_body(a, y, 0, 1, s.data());
+    return ASARF_OK;
+}
+int backend_multilook(const MultilookArgs& a, void*) {
+    for (int y = 0; y < a.out_y; ++y) multilook_row_body(a, y, 0, 1);
+    return ASARF_OK;
+}
+int backend_rsl(const RslArgs& a, long long n, void*) {
+    for (long long i = 0; i < n; ++i) rsl_item(a, i);
+    return ASARF_OK;
+}
+int backend_srgr(const SrgrArgs& a, long long n, void*) {
+    for (long long i = 0; i < n; ++i) srgr_item(a, i);
+    return ASARF_OK;
+}
+
 void* mem_alloc(size_t bytes) { return std::calloc(1, bytes ? bytes : 1); }
 void mem_free(void* p) { std::free(p); }
 int mem_h2d(void* dst, const void* src, size_t n, void*) {

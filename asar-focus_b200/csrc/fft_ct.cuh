@@ -37,7 +37,7 @@ ASARF_CT_SCHEDULE(8192, 512, 8, 8, 8, 8, 2);
 constexpr int kCtLengths[] = {768, 1024, 1536, 2048, 3072, 4096, 6144, 8192};
 
 template <int L, int I>
-constexpr int ct_span() {
+ASARF_HD constexpr int ct_span() {
     int m = L;
     for (int k = 0; k <= I; ++k) m /= CtSchedule<L>::r[k];
     return m;

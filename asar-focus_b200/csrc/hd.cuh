@@ -115,6 +115,14 @@ ASARF_HD ASARF_INLINE unsigned int fdiv_u(unsigned int n, const FastDiv& f) {
 #endif
 }
 
+ASARF_HD ASARF_INLINE float qnan_f() {
+#if defined(__CUDA_ARCH__)
+    return __int_as_float(0x7fc00000);
+#else
+    return __builtin_nanf("");
+#endif
+}
+
 // sin(pi x) with exact argument reduction (CUDA sinpif; FP64 on the host).
 ASARF_HD ASARF_INLINE float sinpi_f32(float x) {
 #if defined(__CUDA_ARCH__)

@@ -12,6 +12,7 @@
 #include "asarf.h"
 #include "backend.h"
 #include "bodies.cuh"
+#include "internal.h"
 
 namespace asarf {
 
@@ -276,10 +277,28 @@ static double fft_cost(int n) {
     return c * n;
 }
 
-static bool smooth(int n) {
+bool smooth(int n) {
     for (int p : {2, 3, 5, 7})
         while (n % p == 0) n /= p;
     return n == 1;
+}
+
+void matched_filter_table(const std::complex<float>* chirp, int nc, const HostFft& fft, std::vector<float2>& mf) {
+    // conj(DFT_L(replica)) / L in FP64, stored in the forward transform's digit-reversed order
+    const int L = fft.plan.n;
+    mf.assign(L, make_float2(0.0f, 0.0f));
+    std::vector<std::complex<double>> w(L);
+    for (int m = 0; m < L; ++m) w[m] = std::polar(1.0, -2.0 * kPi * m / L);
+    for (int pos = 0; pos < L; ++pos) {
+        const int k = fft.drev[pos];
+        std::complex<double> acc(0.0, 0.0);
+        for (int n = 0; n < nc; ++n) {
+            const long long idx = (static_cast<long long>(n) * k) % L;
+            acc += std::complex<double>(chirp[n].real(), chirp[n].imag()) * w[idx];
+        }
+        const std::complex<double> h = std::conj(acc) / static_cast<double>(L);
+        mf[pos] = make_float2(static_cast<float>(h.real()), static_cast<float>(h.imag()));
+    }
 }
 
 int32_t fft_size_above(int32_t v) {
@@ -289,13 +308,7 @@ int32_t fft_size_above(int32_t v) {
     return -1;
 }
 
-struct HostFft {
-    FftPlan plan{};
-    std::vector<int> drev;
-    std::vector<float2> tw;
-};
-
-static bool build_fft(int n, HostFft& h) {
+bool build_fft(int n, HostFft& h) {
     auto f = factorize(n);
     if (f.empty() || static_cast<int>(f.size()) > kMaxStages) return false;
     h.plan.n = n;
@@ -328,7 +341,7 @@ static bool build_fft(int n, HostFft& h) {
     return true;
 }
 
-static int choose_rc_len(int nr) {
+int choose_rc_len(int nr) {
     // a compile-time-scheduled length when one is close above (within 1.5x)
     for (int L : kCtLengths)
         if (L >= nr && 2 * L <= 3 * nr) return L;
@@ -576,22 +589,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     // chirp matched filter in the forward transform's output order, scaled by 1/L
     std::vector<std::complex<float>> chirp;
     generate_chirp(s.chirp_kr, s.range_sampling_rate, p->nc, s.apply_window != 0, p->rc_len, chirp);
-    std::vector<float2> mf(p->rc_len);
-    {
-        const int L = p->rc_len;
-        std::vector<std::complex<double>> w(L);
-        for (int m = 0; m < L; ++m) w[m] = std::polar(1.0, -2.0 * kPi * m / L);
-        for (int pos = 0; pos < L; ++pos) {
-            const int k = p->rc.drev[pos];
-            std::complex<double> acc(0.0, 0.0);
-            for (int n = 0; n < p->nc; ++n) {
-                const long long idx = (static_cast<long long>(n) * k) % L;
-                acc += std::complex<double>(chirp[n].real(), chirp[n].imag()) * w[idx];
-            }
-            const std::complex<double> h = std::conj(acc) / static_cast<double>(L);
-            mf[pos] = make_float2(static_cast<float>(h.real()), static_cast<float>(h.imag()));
-        }
-    }
+    std::vector<float2> mf;
+    matched_filter_table(chirp.data(), p->nc, p->rc, mf);
 
     // results-window variants (CalcResultsWindow, main_flow.cc:155-201) and their tails
     const int max_ap = max_aperture_pixels(s);

@@ -119,6 +119,41 @@ __global__ void __launch_bounds__(512) k_tail(TailArgs a, unsigned int* err) {
     tail_body(a, blockIdx.x, threadIdx.x, blockDim.x, smem_tail, err);
 }
 
+template <class Args, void (*Item)(const Args&, long long)>
+__global__ void __launch_bounds__(256) k_items(Args a, long long n) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        Item(a, i);
+}
+
+ASARF_HD ASARF_INLINE void zero_nan_item(float2* const& img, long long i) {
+    float2 v = img[i];
+    if (is_nan_f(v.x)) v.x = 0.0f;
+    if (is_nan_f(v.y)) v.y = 0.0f;
+    img[i] = v;
+}
+
+__global__ void __launch_bounds__(256) k_img_moments(ImgMomentsArgs a) {
+    __shared__ double red[12 * 256];
+    img_moments_body(a, blockIdx.x, threadIdx.x, blockDim.x, red);
+}
+
+__global__ void __launch_bounds__(256) k_accc(AcccArgs a) { accc_body(a, blockIdx.x, threadIdx.x, blockDim.x); }
+
+__global__ void __launch_bounds__(512) k_rc_rows(RcRowsArgs a) {
+    extern __shared__ float2 smem_rcr[];
+    rc_rows_body(a, blockIdx.x, threadIdx.x, blockDim.x, smem_rcr);
+}
+
+__global__ void __launch_bounds__(256) k_multilook(MultilookArgs a) {
+    multilook_row_body(a, blockIdx.x, threadIdx.x, blockDim.x);
+}
+
+int grid_for(long long n) {
+    long long g = (n + 255) / 256;
+    return static_cast<int>(g < 148 * 32 ? (g > 0 ? g : 1) : 148 * 32);
+}
+
 int check_launch(const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(ASARF_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
@@ -231,6 +266,45 @@ int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err,
     if (rc) return rc;
     k_tail<<<rows, sh.threads, sh.smem, S(stream)>>>(a, err);
     return check_launch("tail");
+}
+
+int backend_decode(const DecodeArgs& a, long long n, void* stream) {
+    k_items<DecodeArgs, decode_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);
+    return check_launch("decode");
+}
+int backend_img_moments(const ImgMomentsArgs& a, int blocks, void* stream) {
+    k_img_moments<<<blocks, 256, 0, S(stream)>>>(a);
+    return check_launch("img_moments");
+}
+int backend_iq_apply(const IqApplyArgs& a, long long n, void* stream) {
+    k_items<IqApplyArgs, iq_apply_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);
+    return check_launch("iq_apply");
+}
+int backend_zero_nans(float2* img, long long n, void* stream) {
+    k_items<float2*, zero_nan_item><<<grid_for(n), 256, 0, S(stream)>>>(img, n);
+    return check_launch("zero_nans");
+}
+int backend_accc(const AcccArgs& a, int blocks, void* stream) {
+    k_accc<<<blocks, 256, 0, S(stream)>>>(a);
+    return check_launch("accc");
+}
+int backend_rc_rows(const RcRowsArgs& a, int rows, LaunchShape sh, void* stream) {
+    int rc = ensure_smem(k_rc_rows, sh.smem, "rc_rows");
+    if (rc) return rc;
+    k_rc_rows<<<rows, sh.threads, sh.smem, S(stream)>>>(a);
+    return check_launch("rc_rows");
+}
+int backend_multilook(const MultilookArgs& a, void* stream) {
+    k_multilook<<<a.out_y, 256, 0, S(stream)>>>(a);
+    return check_launch("multilook");
+}
+int backend_rsl(const RslArgs& a, long long n, void* stream) {
+    k_items<RslArgs, rsl_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);
+    return check_launch("rsl");
+}
+int backend_srgr(const SrgrArgs& a, long long n, void* stream) {
+    k_items<SrgrArgs, srgr_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);
+    return check_launch("srgr");
 }
 
 void* mem_alloc(size_t bytes) {

@@ -158,4 +158,74 @@ struct TailArgs {
     int out_pitch;
 };
 
+// ------------------------------------------------------------------ per-stage entry points
+// (the reference's sar/ functions one by one, on its padded complex image layout)
+
+struct DecodeArgs {
+    const uint8_t* raw;
+    long long line_bytes;
+    int spl, lines, nr;
+    const uint16_t* swst;
+    int min_swst;
+    float2* img;
+    long long stride;   // complex elements per image row
+};
+
+// NaN-aware moment partials of rows [row0, row0 + rows) per block: data region x < x_size
+// and padding region x_size <= x < x_stride, 12 doubles per block:
+// n, sI, sQ, sII, sQQ, sIQ (data) then the same six for the padding.
+struct ImgMomentsArgs {
+    const float2* img;
+    int x_size, y_size, x_stride;
+    int rows_per_block;
+    double* partial;    // [blocks][12]
+    float mean_i, mean_q;   // second pass: sums of (I - mean)^2, (Q - mean)^2 over the data region
+    int centered;
+};
+
+struct IqApplyArgs {
+    float2* img;
+    int x_stride, y_size;
+    float dc_i, dc_q, gain, sin_c, cos_c;
+};
+
+struct AcccArgs {
+    const float2* img;
+    int x_size, y_size, x_stride;
+    int step, nblk, rows_per_block;
+    double* partial;    // [blocks][nblk][2]
+};
+
+struct RcRowsArgs {
+    float2* img;          // in place, rows y < y_size
+    long long stride;
+    int nr, nk, x_zero_end;  // inputs x < nr; keep x < nk; zero [nk, x_zero_end)
+    FftPlan plan;
+    const float2* mf;
+};
+
+struct MultilookArgs {
+    const float2* slc;
+    int x_size, in_y, out_y;
+    float ratio;
+    float* out;
+};
+
+struct RslArgs {
+    float* img;
+    int range_size, az_size;
+    double slant_first, range_spacing, ref_range;
+};
+
+struct SrgrArgs {
+    const float* in;
+    int in_x, y_size, out_x;
+    float grsr[5];
+    float range_spacing, ground_spacing;
+    float* out;
+    int* start;           // optional index map
+    float* frac;
+    unsigned int* err;
+};
+
 }  // namespace asarf

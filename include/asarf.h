@@ -201,6 +201,90 @@ int asarf_srgr_polynomial(const asarf_scene* scene, double slant_first, int32_t 
 /* GetOptimalFFTSizes().upper_bound(v) (cuda_util/cufft_plan.cc:147-181, main.cc:217,223). */
 int32_t asarf_fft_size_above(int32_t v);
 
+/* ---------------------------------------------------------------------------------------
+ * Per-stage entry points: the reference's sar/ functions one at a time, for a caller that
+ * keeps the reference's own pipeline (main.cc) and swaps stages.  Images use the layout of
+ * DevicePaddedImage (cuda_util/device_padded_image.cuh:13-27): complex float
+ * [y_stride][x_stride] on the device, data block [0, y_size) x [0, x_size) at the top left.
+ * Like the reference functions these allocate their own temporaries and synchronise
+ * `stream` before returning; the planned asarf_focus path above is the fused, allocation-
+ * free form of the same chain.
+ * ------------------------------------------------------------------------------------- */
+
+/* SARResults fields written by RawDataCorrection (sar/sar_metadata.h:46-55). */
+typedef struct asarf_iq_results {
+    double dc_i, dc_q;         /* CalcMean over the data block, float as the reference keeps it */
+    double iq_gain;            /* sqrt(sum I^2 / sum Q^2) after the DC step */
+    double phase_error;        /* degrees */
+    double stddev_i, stddev_q; /* CalcStdDev over the data block */
+} asarf_iq_results;
+
+/* The SARMetadata fields RangeDopplerAlgorithm reads (sar/range_doppler_algorithm.cu:340-360). */
+typedef struct asarf_rda_params {
+    double prf;
+    double wavelength;
+    double range_spacing;
+    double slant_range_first;
+    double az_bw_frac;
+    double vr_poly[3];         /* results.Vr_poly, highest power first */
+    double dc_poly[3];         /* results.doppler_centroid_poly, highest power first */
+} asarf_rda_params;
+
+/* ConvertErsImSamplesToComplexKernel (envisat_format/src/envisat_format_kernels.cu:116-134)
+ * with the NaN pre-fill of main_flow.cc:537-540: raw byte I/Q records -> complex rows of
+ * `range_size` samples, shifted right by 4*(swst[y]-min_swst) (d_swst may be NULL), samples
+ * outside the record NaN.  Writes columns [0, range_size) of `lines` rows of d_img. */
+int asarf_convert_ers_samples(const uint8_t* d_raw, int32_t raw_line_bytes, int32_t samples_per_line, int32_t lines,
+                              const uint16_t* d_swst, int32_t min_swst, void* d_img, int64_t img_stride,
+                              int32_t range_size, void* stream);
+/* RawDataCorrection (sar/iq_correction.cu:188-274): means and deviations over the data
+ * block (NaN samples skipped, divided by n_total_samples; <= 0 means x_size*y_size), then
+ * DC, gain and phase correction applied over x < x_stride, y < y_size with the gain and
+ * phase statistics taken over that same region, as the reference does. */
+int asarf_raw_data_correction(void* d_img, int32_t x_size, int32_t y_size, int32_t x_stride, int32_t y_stride,
+                              int64_t n_total_samples, asarf_iq_results* results, void* stream);
+/* DevicePaddedImage::ZeroNaNs (cuda_util/device_padded_image.cu:69-85, 322-329). */
+int asarf_zero_nans(void* d_img, int32_t x_stride, int32_t y_stride, void* stream);
+/* CalculateDopplerCentroid (sar/fractional_doppler_centroid.cu:98-139): ACCC phase over
+ * 32 range blocks of x_size/32 columns (the last one may reach into the padding, as in the
+ * reference), quadratic fit of the block centroids; poly highest power first.  Pair sums
+ * are FP64 in a fixed order (the reference sums float partials). */
+int asarf_doppler_centroid(const void* d_img, int32_t x_size, int32_t y_size, int32_t x_stride, double prf,
+                           double poly[3], void* stream);
+/* RangeCompression (sar/range_compression.cu:57-111) in place: chirp_padded is
+ * ChirpInfo::padded_windowed_data (interleaved re/im, chirp_len = x_stride complex samples,
+ * else "Range padding and chirp size mismatch"); rows y < y_size keep x < x_size -
+ * chirp_samples compressed samples and are zero from there to x_stride.  *new_x_size gets
+ * the new XSize.  The range FFT length is chosen freely (>= x_size): the kept samples do
+ * not depend on it. */
+int asarf_range_compression(void* d_img, int32_t x_size, int32_t y_size, int32_t x_stride, const float* chirp_padded,
+                            int32_t chirp_len, int32_t chirp_samples, int32_t* new_x_size, void* stream);
+/* RangeDopplerAlgorithm (sar/range_doppler_algorithm.cu:312-407): azimuth FFT over all
+ * y_stride rows of columns x < x_size (in place on d_src, which the reference also
+ * consumes), 16-tap RCMC into d_out, azimuth matched filter, inverse FFT scaled by
+ * 1/y_stride.  d_out (same shape) holds the focused block [0, y_size) x [0, x_size) and
+ * zeros elsewhere (the reference leaves unscaled transform values in rows >= y_size).
+ * y_stride must factor into 2, 3, 5 and 7. */
+int asarf_range_doppler(const asarf_rda_params* prm, void* d_src, void* d_out, int32_t x_size, int32_t y_size,
+                        int32_t x_stride, int32_t y_stride, void* stream);
+/* AzimuthMultiLook / TimeDomainAzimuthLook (sar/az_multilook.cu:25-98) on a contiguous
+ * complex [y_size][x_size] SLC: d_out float [out_y][x_size], out_y = round(y_size / ratio),
+ * ratio = float(12.5 / azimuth_spacing).  d_out must hold that many rows. */
+int asarf_azimuth_multilook(const void* d_slc, int32_t x_size, int32_t y_size, double azimuth_spacing, float* d_out,
+                            int32_t* out_y, void* stream);
+/* RangeSpreadingLossCorrection (sar/range_spreading_loss.cu:29-68) in place on a float
+ * [azimuth_size][range_size] image. */
+int asarf_range_spreading_loss(float* d_img, int32_t range_size, int32_t azimuth_size, double slant_range_first,
+                               double range_spacing, double reference_range, void* stream);
+/* SrGrInterpolation (sar/srgr.cu:49-71) with the polynomial of asarf_srgr_polynomial:
+ * float [y_size][in_x] slant rows -> float [y_size][out_x] ground rows at 12.5 m.  An index
+ * outside the slant row (the reference reads past it) is clamped to the last pair. */
+int asarf_srgr(const float* d_in, int32_t in_x, int32_t y_size, const double grsr_poly[5], double range_spacing,
+               int32_t out_x, float* d_out, void* stream);
+/* The per-column (start index, fraction) map SrGrInterpolation computes, for inspection. */
+int asarf_srgr_index(const double grsr_poly[5], double range_spacing, int32_t out_x, int32_t* d_start, float* d_frac,
+                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif
