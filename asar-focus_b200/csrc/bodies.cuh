@@ -531,19 +531,22 @@ ASARF_HD ASARF_INLINE ColParams az_col_params(const AzRdArgs& a, int x) {
     float dcp[3] = {a.state->dc_poly32[0], a.state->dc_poly32[1], a.state->dc_poly32[2]};
     float vrp[3] = {a.vr_poly[0], a.vr_poly[1], a.vr_poly[2]};
     cp.dc = polyval_f32(dcp, xf);
-    cp.vr = polyval_f32(vrp, xf);
+    const float vr = polyval_f32(vrp, xf);
     const float step = a.bin_step;
     const float dc_steps = roundf(fdiv_rn(cp.dc, step));
     cp.dc_off = fmul_rn(dc_steps, step);
-    cp.r0 = a.slant + static_cast<double>(x) * a.range_spacing;
-    cp.inv_dr = 1.0 / a.range_spacing;
-    const float kav = fmul_rn(fmul_rn(2.0f, cp.vr), cp.vr);
-    cp.ka = static_cast<float>(static_cast<double>(kav) / (static_cast<double>(a.lambda) * cp.r0));
+    const double r0 = a.slant + static_cast<double>(x) * a.range_spacing;
+    cp.r0_dr = r0 / a.range_spacing;
+    const float kav = fmul_rn(fmul_rn(2.0f, vr), vr);
+    cp.ka = static_cast<float>(static_cast<double>(kav) / (static_cast<double>(a.lambda) * r0));
     const float half = fmul_rn(a.prf, 0.5f);
     cp.cut_hi = fma_rn(half, a.frac, cp.dc_off);
     cp.cut_lo = fma_rn(-half, a.frac, cp.dc_off);
-    cp.den = fmul_rn(fmul_rn(8.0f, cp.vr), cp.vr);
+    cp.den = fmul_rn(fmul_rn(8.0f, vr), vr);
     cp.dc_off_ka = fdiv_rn(cp.dc_off, cp.ka);
+    cp.rden = fdiv_rn(1.0f, cp.den);
+    cp.rka = fdiv_rn(1.0f, cp.ka);
+    cp.pad = 0.0f;
     return cp;
 }
 
@@ -567,25 +570,18 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
     const float prf = a.prf;
     const float half = a.half_prf;
     const float bf = bin_frequency(f, a.az_pad, a.bin_step);
-    // --- azimuth matched filter band: outside it the reference writes zero whatever RCMC gave
-    float absf = bf;
-    if (cp.dc < 0.0f) {
-        if (bf > fadd_rn(half, cp.dc)) absf = fsub_rn(absf, prf);
-    } else if (cp.dc > 0.0f) {
-        if (absf < fadd_rn(-half, cp.dc)) absf = fadd_rn(absf, prf);
-    }
-    if (absf < cp.cut_lo || absf > cp.cut_hi) return make_float2(0.0f, 0.0f);
-    // --- RCMC (aliased frequency, range walk)
+    // --- aliased frequency (the same test decides the matched-filter band and the RCMC walk)
     float fn = bf;
     if (cp.dc < 0.0f) {
-        if (fn > fadd_rn(half, cp.dc)) fn = fsub_rn(fn, prf);
+        if (bf > fadd_rn(half, cp.dc)) fn = fsub_rn(fn, prf);
     } else if (cp.dc > 0.0f) {
         if (fn < fadd_rn(-half, cp.dc)) fn = fadd_rn(fn, prf);
     }
+    // outside the processed band the reference writes zero whatever RCMC gave
+    if (fn < cp.cut_lo || fn > cp.cut_hi) return make_float2(0.0f, 0.0f);
+    // --- RCMC: walk = lambda^2 fn^2 / (8 Vr^2) [float, IEEE divide] * R0 [double] / range spacing
     const float num = fmul_rn(fmul_rn(fmul_rn(a.lambda, a.lambda), fn), fn);
-    double dr = static_cast<double>(fdiv_rn(num, cp.den));
-    dr *= cp.r0;
-    const float shift = static_cast<float>(dr * cp.inv_dr);
+    const float shift = static_cast<float>(static_cast<double>(div_by_recip_rn(num, cp.den, cp.rden)) * cp.r0_dr);
     const int walk = static_cast<int>(roundf(shift));
     const int calc_x = x + walk;
     float2 out = make_float2(0.0f, 0.0f);
@@ -594,42 +590,39 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
         if (first < 0 || first + kRcmcTaps > a.wt) {
             atomic_or_u32(err_flag, kErrRcmcHalo);
         } else {
+            // Windowed sinc at off - i, off = shift - walk + 8 in [7.5, 8.5]:
+            // sin(pi (off - i)) = (-1)^i sin(pi off), and the common factor sin(pi off) / pi
+            // cancels in the normalised sum, leaving weights (-1)^i W_i / (off - i).
             const float off = fadd_rn(fsub_rn(shift, static_cast<float>(walk)), static_cast<float>(kRcmcTaps / 2));
-            const float pi = 3.14159265358979323846f;
-            // sin(pi (off - i)) = (-1)^i sin(pi off): one sinpi per output instead of one sinf per tap;
-            // the denominators pi (off - i) are rounded exactly as the reference rounds them
-            const float s_off = sinpi_f32(off);
-            constexpr float kWin[kRcmcTaps] = ASARF_BLACKMAN16;
-            float si = 0.0f, sq = 0.0f, nrm = 0.0f;
+            if (off == static_cast<float>(kRcmcTaps / 2)) {
+                out = srow[first + kRcmcTaps / 2];  // integer shift: sinc is a unit impulse
+            } else {
+                constexpr float kWin[kRcmcTaps] = ASARF_BLACKMAN16;
+                float si = 0.0f, sq = 0.0f, nrm = 0.0f;
 #pragma unroll
-            for (int i = 0; i < kRcmcTaps; ++i) {
-                const float arg = fsub_rn(off, static_cast<float>(i));
-                const float q = fast_div((i & 1) ? -s_off : s_off, fmul_rn(pi, arg));
-                const float sinc = (arg != 0.0f) ? q : 1.0f;
-                const float wgt = fmul_rn(kWin[i], sinc);
-                const float2 d = srow[first + i];
-                si = fma_rn(d.x, wgt, si);
-                sq = fma_rn(d.y, wgt, sq);
-                nrm = fadd_rn(nrm, wgt);
-            }
-            if (nrm != 0.0f) {
-                const float inv = fast_div(1.0f, nrm);
-                out = make_float2(fmul_rn(si, inv), fmul_rn(sq, inv));
+                for (int i = 0; i < kRcmcTaps; ++i) {
+                    const float wgt = fast_div((i & 1) ? -kWin[i] : kWin[i], fsub_rn(off, static_cast<float>(i)));
+                    const float2 d = srow[first + i];
+                    si = fma_rn(d.x, wgt, si);
+                    sq = fma_rn(d.y, wgt, sq);
+                    nrm = fadd_rn(nrm, wgt);
+                }
+                if (nrm != 0.0f) {
+                    const float inv = fast_div(1.0f, nrm);
+                    out = make_float2(fmul_rn(si, inv), fmul_rn(sq, inv));
+                }
             }
         }
     }
-    // --- matched filter exp(-j pi fc^2 / Ka) * exp(-j 2 pi (dc_off / Ka) f)
+    // --- matched filter exp(-j pi fc^2 / Ka) * exp(-j 2 pi (dc_off / Ka) f), both phases
+    // rounded as the reference rounds them, combined into one reduced exponential
     float fc = fsub_rn(bf, cp.dc_off);
     if (fc > half) fc = fsub_rn(fc, prf);
     else if (fc < -half) fc = fadd_rn(fc, prf);
     const float pi = 3.14159265358979323846f;
-    const float mf_phase = fdiv_rn(fmul_rn(fmul_rn(pi, fc), fc), cp.ka);
-    float s1, c1, s2, c2;
-    sincosf(mf_phase, &s1, &c1);
+    const float mf_phase = div_by_recip_rn(fmul_rn(fmul_rn(pi, fc), fc), cp.ka, cp.rka);
     const float sh_phase = fmul_rn(fmul_rn(fmul_rn(2.0f, pi), cp.dc_off_ka), bf);
-    sincosf(sh_phase, &s2, &c2);
-    const float2 mf = cmul(make_float2(c1, -s1), make_float2(c2, -s2));
-    return cmul(out, mf);
+    return cmul(out, expj_neg_sum(mf_phase, sh_phase));
 }
 
 ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s, float2* tmp,

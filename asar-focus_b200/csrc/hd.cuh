@@ -85,6 +85,57 @@ ASARF_HD ASARF_INLINE float fsub_rn(float a, float b) {
 #endif
 }
 
+// a / b rounded to nearest, given rb = RN(1 / b): q0 = RN(a rb) is within one ulp of a / b,
+// the residual a - b q0 is exact in one FMA, and RN(q0 + residual * rb) is the correctly
+// rounded quotient (Markstein, IBM J. Res. Dev. 34(1), 1990; the theorem in round-to-nearest
+// binary arithmetic, no overflow or underflow).  Three operations when b is reused.
+ASARF_HD ASARF_INLINE float div_by_recip_rn(float a, float b, float rb) {
+    const float q0 = fmul_rn(a, rb);
+    const float r = fma_rn(-q0, b, a);
+    return fma_rn(r, rb, q0);
+}
+
+// sin and cos of x in [-pi, pi] from the hardware approximation (absolute error below
+// 2^-21.4 there on the device); the host emulation evaluates them in FP64.
+ASARF_HD ASARF_INLINE void sincos_reduced(float x, float* s, float* c) {
+#if defined(__CUDA_ARCH__)
+    __sincosf(x, s, c);
+#else
+    *s = static_cast<float>(__builtin_sin(static_cast<double>(x)));
+    *c = static_cast<float>(__builtin_cos(static_cast<double>(x)));
+#endif
+}
+
+ASARF_HD ASARF_INLINE float rint_f(float x) {
+#if defined(__CUDA_ARCH__)
+    return rintf(x);
+#else
+    return __builtin_rintf(x);
+#endif
+}
+
+// exp(-j (a + b)) for float phases a, b in radians with |a + b| < 2^20.  The sum is kept
+// exactly as a float pair (Knuth's two-sum), reduced by k = rint((a + b) / 2 pi) against a
+// two-part 2 pi (Cody & Waite): s - k * A is exact (both are multiples of ulp(A) = 2^-21 once
+// |s| >= 4, Sterbenz below that, and the difference is under 4), so the reduced angle carries
+// only the roundings of the two small terms.
+ASARF_HD ASARF_INLINE float2 expj_neg_sum(float a, float b) {
+    constexpr double kTwoPi = 6.283185307179586476925286766559;
+    constexpr float kTwoPiA = static_cast<float>(kTwoPi);
+    constexpr float kTwoPiB = static_cast<float>(kTwoPi - static_cast<double>(kTwoPiA));
+    constexpr float kInvTwoPi = static_cast<float>(1.0 / kTwoPi);
+    const float s = fadd_rn(a, b);
+    const float bb = fsub_rn(s, a);
+    const float e = fadd_rn(fsub_rn(a, fsub_rn(s, bb)), fsub_rn(b, bb));
+    const float k = rint_f(fmul_rn(s, kInvTwoPi));
+    float r = fma_rn(-k, kTwoPiA, s);
+    r = fma_rn(-k, kTwoPiB, r);
+    r = fadd_rn(r, e);
+    float sn, cs;
+    sincos_reduced(r, &sn, &cs);
+    return make_float2(cs, -sn);
+}
+
 // Division by a loop-invariant divisor d < 2^16 of n < 2^16 without a hardware divide:
 // q = umulhi(n, ceil(2^32 / d)) (exact while n * (m d - 2^32) < 2^32), or a shift when d is
 // a power of two.

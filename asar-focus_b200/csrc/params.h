@@ -111,9 +111,12 @@ struct AzStridedArgs {
     int n1_box;           // rows per TMA box (n1 split into n1 / n1_box boxes of <= 256 rows)
 };
 
+// Per range column constants of the range-Doppler block.
 struct ColParams {
-    float dc, vr, dc_off, ka, cut_lo, cut_hi, den, dc_off_ka;
-    double r0, inv_dr;
+    float dc, dc_off, ka, cut_lo, cut_hi, den, dc_off_ka;
+    float rden, rka;      // RN(1 / den), RN(1 / ka) for the exact divisions
+    float pad;
+    double r0_dr;         // R0 / range spacing (range walk metres -> pixels)
 };
 
 struct AzRdArgs {

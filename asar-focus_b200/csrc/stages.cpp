@@ -208,7 +208,10 @@ int asarf_range_compression(void* d_img, int32_t x_size, int32_t y_size, int32_t
     a.plan = fft.plan;
     a.plan.tw = tw.as<float2>();
     a.mf = mfd.as<float2>();
-    rc = backend_rc_rows(a, y_size, LaunchShape{512, sizeof(float2) * static_cast<size_t>(L)}, stream);
+    const LaunchShape sh{512, sizeof(float2) * static_cast<size_t>(L)};
+    if (sh.smem > smem_optin_limit())
+        return set_error(ASARF_ERR_INVALID, "range_compression: range FFT of %d samples exceeds shared memory", L);
+    rc = backend_rc_rows(a, y_size, sh, stream);
     if (rc) return rc;
     if (new_x_size) *new_x_size = a.nk;
     return stream_sync(stream);
@@ -335,6 +338,7 @@ int asarf_azimuth_multilook(const void* d_slc, int32_t x_size, int32_t y_size, d
     a.ratio = static_cast<float>(12.5f / azimuth_spacing);
     a.out_y = static_cast<int>(std::round(static_cast<float>(y_size) / a.ratio));
     a.out = d_out;
+    if (a.out_y <= 0) return set_error(ASARF_ERR_INVALID, "azimuth_multilook: no output lines");
     if (out_y) *out_y = a.out_y;
     int rc = backend_multilook(a, stream);
     if (rc) return rc;

@@ -278,7 +278,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "config": {"workload": f"{args.workload}: ERS-like {sc.range_size} range x {sc.azimuth_size} azimuth, "
                                f"{sc.bits}-bit I/Q, 20x20 point grid, DC 250..350 Hz, Vr from 5 orbit vectors",
                    "range_samples": sc.range_size, "azimuth_lines": sc.azimuth_size, "scenes_per_step": world,
-                   "l2": "inputs larger than L2 (raw 314 MB, complex images 1.1 GB each)",
+                   "l2": f"inputs larger than L2 (raw {raw_np.nbytes / 1e6:.0f} MB, complex images "
+                         f"{dims['az_pad'] * dims['nk'] * 8 / 1e9:.2f} GB each)",
                    "parallelism": f"replicas x{world} (independent scenes)",
                    "az_pad": dims["az_pad"], "rc_fft_len": dims["rc_fft_len"]},
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
