@@ -77,7 +77,7 @@ def build_emu(out_dir: str | os.PathLike, force: bool = False) -> Path:
         return out
     out.parent.mkdir(parents=True, exist_ok=True)
     cxx = os.environ.get("CXX", "g++")
-    cmd = [cxx, "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-DASARF_HOST_EMU",
+    cmd = [cxx, "-std=c++17", "-O2", "-ffp-contract=off", "-fno-strict-aliasing", "-fPIC", "-shared", "-DASARF_HOST_EMU",
            f"-I{INC}", f"-I{CSRC}", f"-I{CUDA_INC}", "-x", "c++", str(CSRC / "host.cpp"), "-x", "c++",
            str(CSRC / "stages.cpp"), "-x", "c++", str(CSRC / "emu.cpp"), "-o", str(out)]
     _run(cmd)

@@ -484,7 +484,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
     }
     ASARF_SYNC();
     if (!a.inverse) {
-        fft_forward(a.plan1, s, xt, xt, tid, nthr);
+        fft_forward_pairs(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
             const int k1 = ASARF_LDG(a.drev1 + p);
@@ -500,7 +500,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
             s[t] = cmulc(s[t], ASARF_LDG(a.twn + b * k1));
         }
         ASARF_SYNC();
-        fft_inverse_dif(a.plan1, s, xt, xt, tid, nthr);
+        fft_inverse_dif_pairs(a.plan1, s, xt, xt, tid, nthr);
         const int lo = a.state ? a.state->first_line : 0;
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {
@@ -643,7 +643,7 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     }
     for (int c = tid; c < a.xt; c += nthr) cps[c] = az_col_params(a, x0 + c);
     ASARF_SYNC();
-    fft_forward(a.plan2, s, wt, wt, tid, nthr);
+    fft_forward_pairs(a.plan2, s, wt, wt, tid, nthr);
     // RCMC + matched filter.  Every output (row p, column c) reads taps of row p only, so a
     // row is computed into registers by one warp (lane = column, xt <= 64), the warp
     // synchronises, and writes it back in place: no block-wide barrier per row.
@@ -677,7 +677,7 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
         (void)tmp;
     }
 #endif
-    fft_inverse(a.plan2, s + a.hl, a.xt, wt, tid, nthr);
+    fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr);
     for (int t = tid; t < n2 * a.xt; t += nthr) {
         const int r = static_cast<int>(fdiv_u(t, dxt)), c = t - r * a.xt;
         const int x = x0 + c;

@@ -13,6 +13,15 @@
 
 namespace asarf {
 
+namespace {
+// Shared-memory stand-in with the device's 16-byte vector alignment.
+struct TileBuf {
+    std::vector<float4> v;
+    explicit TileBuf(size_t bytes) : v(bytes / sizeof(float4) + 2) {}
+    float2* data() { return reinterpret_cast<float2*>(v.data()); }
+};
+}  // namespace
+
 int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, int threads, int cols, void*) {
     (void)threads;
     RawStatsSmem sm;
@@ -49,14 +58,14 @@ int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh
 }
 
 int backend_az_strided(const AzStridedArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, void*) {
-    std::vector<float2> s(sh.smem / sizeof(float2) + 1);
+    TileBuf s(sh.smem);
     for (int b = 0; b < nblocks; ++b)
         for (int t = 0; t < tiles; ++t) az_strided_body(a, t, b, 0, 1, s.data(), false);
     return ASARF_OK;
 }
 
 int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void*) {
-    std::vector<float2> buf(sh.smem / sizeof(float2) + 16);
+    TileBuf buf(sh.smem + 128);
     float2* s = buf.data();
     float2* tmp = s + a.n2 * a.wt;
     ColParams* cps = reinterpret_cast<ColParams*>(tmp);

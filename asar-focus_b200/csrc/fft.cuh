@@ -243,6 +243,103 @@ ASARF_HD ASARF_INLINE void fft_stage_dif_inv(float2* s, int n, int S, const Fast
     }
 }
 
+// ----------------------------------------------------------------------------- column pairs
+// The same stages over PAIRS of adjacent columns: one 16-byte shared-memory access moves
+// both columns' samples and one twiddle set serves both butterflies.  Needs ldc even, the
+// tile base 16-byte aligned and an even column count.  TW_FIRST selects decimation in time
+// (twiddle, then DFT); INV selects the inverse DFT sign and conjugated twiddles.
+template <int R, bool INV, bool TW_FIRST>
+ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv& sdiv, int npair, const FastDiv& pdiv,
+                                          int ldc, const float2* __restrict__ tw, int tid, int nthr) {
+    const int M = S * R;
+    const int items = (n / R) * npair;
+    const int tw_step = n / M;
+    const int st = (S * ldc) >> 1;  // float4 units
+    for (int t = tid; t < items; t += nthr) {
+        const int bj = static_cast<int>(fdiv_u(t, pdiv));
+        const int cp = t - bj * npair;
+        const int b = static_cast<int>(fdiv_u(bj, sdiv));
+        const int j = bj - b * S;
+        float4* p = reinterpret_cast<float4*>(s + (b * M + j) * ldc) + cp;
+        float2 u[R], v[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const float4 q = p[m * st];
+            u[m] = make_float2(q.x, q.y);
+            v[m] = make_float2(q.z, q.w);
+        }
+        if (TW_FIRST && j != 0) {
+            const float2 w1 = ASARF_LDG(tw + j * tw_step);
+            float2 w = w1;
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                u[q] = INV ? cmulc(u[q], w) : cmul(u[q], w);
+                v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
+                w = cmul(w, w1);
+            }
+        }
+        dft<R, INV>(u);
+        dft<R, INV>(v);
+        if (!TW_FIRST && j != 0) {
+            const float2 w1 = ASARF_LDG(tw + j * tw_step);
+            float2 w = w1;
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                u[q] = INV ? cmulc(u[q], w) : cmul(u[q], w);
+                v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
+                w = cmul(w, w1);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) p[m * st] = make_float4(u[m].x, u[m].y, v[m].x, v[m].y);
+    }
+}
+
+template <bool INV, bool TW_FIRST>
+ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int npair,
+                                                   const FastDiv& pdiv, int ldc, const float2* __restrict__ tw,
+                                                   int tid, int nthr) {
+    switch (R) {
+        case 2: fft_stage_pair<2, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
+        case 3: fft_stage_pair<3, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
+        case 4: fft_stage_pair<4, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
+        case 5: fft_stage_pair<5, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
+        case 7: fft_stage_pair<7, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
+        default: fft_stage_pair<8, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
+    }
+}
+
+// Column-pair forms of fft_forward / fft_inverse / fft_inverse_dif (ncol and ldc even).
+ASARF_HD ASARF_INLINE void fft_forward_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    const int npair = ncol >> 1;
+    const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
+    for (int i = 0; i < p.nst; ++i) {
+        fft_stage_pair_dispatch<false, false>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
+                                              nthr);
+        ASARF_SYNC();
+    }
+}
+
+ASARF_HD ASARF_INLINE void fft_inverse_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    const int npair = ncol >> 1;
+    const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
+    for (int i = p.nst - 1; i >= 0; --i) {
+        fft_stage_pair_dispatch<true, true>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
+                                            nthr);
+        ASARF_SYNC();
+    }
+}
+
+ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+    const int npair = ncol >> 1;
+    const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
+    for (int i = 0; i < p.nst; ++i) {
+        fft_stage_pair_dispatch<true, false>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
+                                             nthr);
+        ASARF_SYNC();
+    }
+}
+
 template <bool INV>
 ASARF_HD ASARF_INLINE void fft_stage_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int ncol,
                                               const FastDiv& cdiv, int ldc, const float2* __restrict__ tw, int tid,

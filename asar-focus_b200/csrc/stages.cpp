@@ -296,6 +296,7 @@ int asarf_range_doppler(const asarf_rda_params* prm, void* d_src, void* d_out, i
     d.xt = 64;
     d.hl = kRcmcTaps / 2;
     d.hr = kRcmcTaps / 2 + static_cast<int>(std::ceil(walk)) + 2;
+    if ((d.xt + d.hl + d.hr) & 1) ++d.hr;  // column-pair transforms need an even tile width
     d.wt = d.xt + d.hl + d.hr;
     d.prf = static_cast<float>(prm->prf);
     d.bin_step = d.prf / static_cast<float>(N);
