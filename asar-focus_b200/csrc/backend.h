@@ -14,7 +14,8 @@ struct LaunchShape {
     size_t smem;
 };
 
-int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, int threads, int cols, void* stream);
+// grid (ceil(nr / kStatsCols), ceil(na / lines_per_cta)), kStatsCols threads
+int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, void* stream);
 int backend_finalize(const FinalizeArgs& a, void* stream);
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void* stream);
 int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream);

@@ -99,168 +99,283 @@ ASARF_HD inline bool polyfit_qr(const double* x, const double* y, int m, int deg
 // and of CalculateDopplerCentroid (sar/fractional_doppler_centroid.cu:33-69: lag-1
 // azimuth correlation per range block): the IQ correction is affine in the raw bytes,
 // so every sum the reference takes over corrected floats is a closed form of these.
-// Block (bx, by) covers columns [bx*cols, (bx+1)*cols) and lines [by*L, (by+1)*L).
+// Block (bx, by) covers kStatsCols work units and lines [by*L, (by+1)*L).  A unit is either
+// one column (general path) or, when the raw base and line stride are 8-byte aligned, a group
+// of 4 adjacent columns inside one Doppler block (quad path: one 8-byte window per line,
+// byte-lane dot products for all sums).  Either way every sum a thread keeps belongs to a
+// single Doppler block, and kStatsBatch lines are loaded before any is consumed.
+constexpr int kStatsCols = 256;
+constexpr int kStatsBatch = 8;
+constexpr int kStatsMaxLines = 256;
+
 struct RawStatsSmem {
     unsigned long long mom[6];
     unsigned long long lag[kMaxDcBlocks][9];
+    int off[kStatsMaxLines + 1];  // SWST shift of the block's lines (and the line before)
 };
 
-ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by, int tid, int nthr, int cols,
+// Host side: work units and grid width of the statistics kernel for this raw buffer.
+inline int raw_stats_grid_x(RawStatsArgs& a, const void* raw) {
+    a.gpb = (a.dc_step + 3) / 4;
+    a.quad = (reinterpret_cast<uintptr_t>(raw) % 8 == 0 && a.line_bytes % 8 == 0) ? 1 : 0;
+    const int units = a.quad ? a.nblk * a.gpb : a.nr;
+    return (units + kStatsCols - 1) / kStatsCols;
+}
+
+// sum over the four byte lanes of a * b, plus c
+ASARF_HD ASARF_INLINE unsigned int dp4(unsigned int a, unsigned int b, unsigned int c) {
+#if defined(__CUDA_ARCH__)
+    return __dp4a(a, b, c);
+#else
+    for (int k = 0; k < 32; k += 8) c += ((a >> k) & 0xffu) * ((b >> k) & 0xffu);
+    return c;
+#endif
+}
+
+ASARF_HD ASARF_INLINE unsigned int funnel_r(unsigned int lo, unsigned int hi, unsigned int sh) {
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_r(lo, hi, sh);
+#else
+    return sh == 0 ? lo : static_cast<unsigned int>(((static_cast<unsigned long long>(hi) << 32) | lo) >> sh);
+#endif
+}
+
+ASARF_HD ASARF_INLINE int popc_u32(unsigned int v) {
+#if defined(__CUDA_ARCH__)
+    return __popc(v);
+#else
+    return __builtin_popcount(v);
+#endif
+}
+
+// Reduce this thread's sums into the block's shared accumulators (lag sums of Doppler block blk).
+ASARF_HD ASARF_INLINE void raw_stats_reduce(RawStatsSmem* sm, bool valid, int blk, unsigned long long mv[6],
+                                            unsigned int lv[9]) {
+#if defined(__CUDA_ARCH__)
+    // every lane of the block runs exactly one unit (kStatsCols == blockDim.x): warp sums first
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        unsigned long long v = mv[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        mv[k] = v;
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
+    }
+    const int bmin = __reduce_min_sync(0xffffffffu, valid ? blk : 0x7fffffff);
+    const int bmax = __reduce_max_sync(0xffffffffu, valid ? blk : -1);
+    if (bmin == bmax) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) lv[q] = __reduce_add_sync(0xffffffffu, valid ? lv[q] : 0u);
+        if ((threadIdx.x & 31) == 0)
+            for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[bmin][q], lv[q]);
+    } else if (valid) {
+        for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[blk][q], lv[q]);
+    }
+#else
+    for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
+    if (valid)
+        for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[blk][q], lv[q]);
+#endif
+}
+
+// General path: one column per unit, one 2-byte load per line.
+ASARF_HD ASARF_INLINE void raw_stats_column(const RawStatsArgs& a, const RawStatsSmem* sm, int x, int y0, int y1,
+                                            int ys, unsigned long long mv[6], unsigned int lv[9]) {
+    unsigned int cnt = 0, si = 0, sq = 0, sii = 0, sqq = 0, siq = 0;
+    unsigned int l0 = 0, l1 = 0, l2 = 0, l3 = 0, l4 = 0, l5 = 0, l6 = 0, l7 = 0, l8 = 0;
+    unsigned int pi = 0, pq = 0;
+    bool pf = false;
+    const uint8_t* col = a.raw + 2ll * x;
+    for (int yg = ys; yg < y1; yg += kStatsBatch) {
+        unsigned int w[kStatsBatch];
+        bool f[kStatsBatch];
+#pragma unroll
+        for (int u = 0; u < kStatsBatch; ++u) {
+            const int y = yg + u;
+            f[u] = false;
+            w[u] = 0u;
+            if (y < y1) {
+                const int off = sm->off[y - ys];
+                const int i = x - off;
+                if (i >= 0 && i < a.spl) {
+                    f[u] = true;
+                    w[u] = *reinterpret_cast<const uint16_t*>(col + static_cast<long long>(y) * a.line_bytes - 2ll * off);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kStatsBatch; ++u) {
+            const int y = yg + u;
+            if (y >= y1) break;
+            const unsigned int iv = w[u] & 0xffu, qv = w[u] >> 8;
+            if (y >= y0 && f[u]) {
+                cnt += 1;
+                si += iv;
+                sq += qv;
+                sii += iv * iv;
+                sqq += qv * qv;
+                siq += iv * qv;
+                if (y > 0 && pf) {
+                    l0 += 1;
+                    l1 += pi;
+                    l2 += pq;
+                    l3 += iv;
+                    l4 += qv;
+                    l5 += pi * iv;
+                    l6 += pq * qv;
+                    l7 += pi * qv;
+                    l8 += pq * iv;
+                }
+            }
+            pi = iv;
+            pq = qv;
+            pf = f[u];
+        }
+    }
+    mv[0] = cnt, mv[1] = si, mv[2] = sq, mv[3] = sii, mv[4] = sqq, mv[5] = siq;
+    lv[0] = l0, lv[1] = l1, lv[2] = l2, lv[3] = l3, lv[4] = l4, lv[5] = l5, lv[6] = l6, lv[7] = l7, lv[8] = l8;
+}
+
+// Quad path: columns x0 .. x0 + ncol - 1 (ncol <= 4, one Doppler block).  A line's four
+// samples are the 8 bytes (I0 Q0 I1 Q1 | I2 Q2 I3 Q3) at raw + y*line_bytes + 2*(x0 - off); their
+// offset inside an 8-byte word, o = 2*x0 mod 8, is the same on every line (the SWST shift is a
+// multiple of 4 samples), so two aligned 8-byte loads and a funnel shift fetch them.  Samples
+// outside the record or the group are masked to zero bytes, which drop out of every sum.
+ASARF_HD ASARF_INLINE void raw_stats_quad(const RawStatsArgs& a, const RawStatsSmem* sm, int x0, int ncol, int y0,
+                                          int y1, int ys, unsigned long long mv[6], unsigned int lv[9]) {
+    constexpr unsigned int kLo = 0x00ff00ffu, kOnes = 0x01010101u;
+    const unsigned int colbits = (1u << ncol) - 1u;
+    const unsigned int o = static_cast<unsigned int>(2 * x0) & 7u;
+    const unsigned int sh = (o & 2u) * 8u;
+    const bool hi_word = (o & 4u) != 0;
+    unsigned int cnt = 0, si = 0, sq = 0, sii = 0, sqq = 0, siq = 0;
+    unsigned int l0 = 0, l1 = 0, l2 = 0, l3 = 0, l4 = 0, l5 = 0, l6 = 0, l7 = 0, l8 = 0;
+    unsigned int pI0 = 0, pI1 = 0, pQ0 = 0, pQ1 = 0, pfb = 0;
+    const uint8_t* base = a.raw + 2ll * x0 - o;
+    for (int yg = ys; yg < y1; yg += kStatsBatch) {
+        // loads only in this loop (nothing consumes them), so all kStatsBatch lines are in flight
+        uint2 lo[kStatsBatch], hi[kStatsBatch];
+        unsigned int fbv[kStatsBatch];
+        bool vec[kStatsBatch];
+#pragma unroll
+        for (int u = 0; u < kStatsBatch; ++u) {
+            const int y = yg + u;
+            lo[u] = hi[u] = make_uint2(0u, 0u);
+            fbv[u] = 0u;
+            vec[u] = false;
+            if (y < y1) {
+                const int off = sm->off[y - ys];
+                const int i = x0 - off;
+                if (i >= 0 && i + 4 <= a.spl) {
+                    // the whole 8-byte window is inside the record
+                    const uint2* p = reinterpret_cast<const uint2*>(base + static_cast<long long>(y) * a.line_bytes -
+                                                                    2ll * off);
+                    lo[u] = p[0];
+                    if (o != 0u) hi[u] = p[1];
+                    fbv[u] = colbits;
+                    vec[u] = true;
+                } else {
+                    // record edge: sample by sample, words already assembled in lo
+                    const uint8_t* row = a.raw + static_cast<long long>(y) * a.line_bytes;
+                    for (int k = 0; k < ncol; ++k) {
+                        if (i + k < 0 || i + k >= a.spl) continue;
+                        const unsigned int v = *reinterpret_cast<const uint16_t*>(row + 2ll * (i + k));
+                        if (k < 2) lo[u].x |= v << (16 * k);
+                        else lo[u].y |= v << (16 * (k - 2));
+                        fbv[u] |= 1u << k;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kStatsBatch; ++u) {
+            const int y = yg + u;
+            if (y >= y1) break;
+            unsigned int w0u = lo[u].x, w1u = lo[u].y;
+            if (vec[u]) {
+                const unsigned int wa = hi_word ? lo[u].y : lo[u].x;
+                const unsigned int wb = hi_word ? hi[u].x : lo[u].y;
+                const unsigned int wc = hi_word ? hi[u].y : hi[u].x;
+                w0u = funnel_r(wa, wb, sh);
+                w1u = funnel_r(wb, wc, sh);
+            }
+            const unsigned int fb = fbv[u];
+            const unsigned int m0 = ((fb & 1u) ? 0x0000ffffu : 0u) | ((fb & 2u) ? 0xffff0000u : 0u);
+            const unsigned int m1 = ((fb & 4u) ? 0x0000ffffu : 0u) | ((fb & 8u) ? 0xffff0000u : 0u);
+            const unsigned int c0 = w0u & m0, c1 = w1u & m1;
+            const unsigned int I0 = c0 & kLo, I1 = c1 & kLo;
+            const unsigned int Q0 = (c0 >> 8) & kLo, Q1 = (c1 >> 8) & kLo;
+            if (y >= y0) {
+                cnt += static_cast<unsigned int>(popc_u32(fb));
+                si = dp4(I0, kOnes, dp4(I1, kOnes, si));
+                sq = dp4(Q0, kOnes, dp4(Q1, kOnes, sq));
+                sii = dp4(I0, I0, dp4(I1, I1, sii));
+                sqq = dp4(Q0, Q0, dp4(Q1, Q1, sqq));
+                siq = dp4(I0, Q0, dp4(I1, Q1, siq));
+                if (y > 0) {
+                    // pairs (y-1, y) with both samples filled
+                    const unsigned int pb = fb & pfb;
+                    if (pb == fb && pb == pfb) {
+                        l1 = dp4(pI0, kOnes, dp4(pI1, kOnes, l1));
+                        l2 = dp4(pQ0, kOnes, dp4(pQ1, kOnes, l2));
+                        l3 = dp4(I0, kOnes, dp4(I1, kOnes, l3));
+                        l4 = dp4(Q0, kOnes, dp4(Q1, kOnes, l4));
+                    } else {
+                        const unsigned int n0 = ((pb & 1u) ? 0x000000ffu : 0u) | ((pb & 2u) ? 0x00ff0000u : 0u);
+                        const unsigned int n1 = ((pb & 4u) ? 0x000000ffu : 0u) | ((pb & 8u) ? 0x00ff0000u : 0u);
+                        l1 = dp4(pI0 & n0, kOnes, dp4(pI1 & n1, kOnes, l1));
+                        l2 = dp4(pQ0 & n0, kOnes, dp4(pQ1 & n1, kOnes, l2));
+                        l3 = dp4(I0 & n0, kOnes, dp4(I1 & n1, kOnes, l3));
+                        l4 = dp4(Q0 & n0, kOnes, dp4(Q1 & n1, kOnes, l4));
+                    }
+                    l0 += static_cast<unsigned int>(popc_u32(pb));
+                    // products vanish wherever either sample is unfilled (its bytes are zero)
+                    l5 = dp4(pI0, I0, dp4(pI1, I1, l5));
+                    l6 = dp4(pQ0, Q0, dp4(pQ1, Q1, l6));
+                    l7 = dp4(pI0, Q0, dp4(pI1, Q1, l7));
+                    l8 = dp4(pQ0, I0, dp4(pQ1, I1, l8));
+                }
+            }
+            pI0 = I0, pI1 = I1, pQ0 = Q0, pQ1 = Q1, pfb = fb;
+        }
+    }
+    mv[0] = cnt, mv[1] = si, mv[2] = sq, mv[3] = sii, mv[4] = sqq, mv[5] = siq;
+    lv[0] = l0, lv[1] = l1, lv[2] = l2, lv[3] = l3, lv[4] = l4, lv[5] = l5, lv[6] = l6, lv[7] = l7, lv[8] = l8;
+}
+
+ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by, int tid, int nthr,
                                           RawStatsSmem* sm) {
     unsigned long long* flat = &sm->mom[0];
     const int nflat = 6 + a.nblk * 9;
     for (int i = tid; i < 6 + kMaxDcBlocks * 9; i += nthr) flat[i] = 0ull;
-    ASARF_SYNC();
     const int y0 = by * a.lines_per_cta;
     const int y1 = (y0 + a.lines_per_cta < a.na) ? y0 + a.lines_per_cta : a.na;
     const int ys = y0 > 0 ? y0 - 1 : 0;
+    for (int y = ys + tid; y < y1; y += nthr) sm->off[y - ys] = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
+    ASARF_SYNC();
     const FastDiv dstep = make_fastdiv(static_cast<unsigned int>(a.dc_step));
-    // thread item t covers columns x = bx*cols + 4t .. +3 (cols is a multiple of 4*nthr)
-    for (int t = tid; t < cols / 4; t += nthr) {
-        const int xb = bx * cols + 4 * t;
-        const bool xin = xb < a.nr;
-        unsigned int cnt = 0, si = 0, sq = 0, sii = 0, sqq = 0, siq = 0;
-        unsigned int l[4][9];
-        for (int k = 0; k < 4; ++k)
-            for (int q = 0; q < 9; ++q) l[k][q] = 0u;
-        int pi[4] = {0, 0, 0, 0}, pq[4] = {0, 0, 0, 0};
-        bool pf[4] = {false, false, false, false};
-        if (xin) {
-            // lines in groups of 4: the group's loads are issued before any is consumed
-            for (int yg = ys; yg < y1; yg += 4) {
-                uint2 wv[4];
-                int i0v[4];
-                bool vec[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int y = yg + u;
-                    vec[u] = false;
-                    i0v[u] = 0;
-                    wv[u] = make_uint2(0u, 0u);
-                    if (y < y1) {
-                        const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
-                        i0v[u] = xb - off;
-                        vec[u] = a.vec_ok && i0v[u] >= 0 && i0v[u] + 4 <= a.spl && xb + 4 <= a.nr;
-                        if (vec[u])
-                            wv[u] = *reinterpret_cast<const uint2*>(a.raw + static_cast<long long>(y) * a.line_bytes +
-                                                                    2ll * i0v[u]);
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int y = yg + u;
-                    if (y >= y1) break;
-                    const int i0 = i0v[u];
-                    int iv[4], qv[4];
-                    bool f[4];
-                    if (vec[u]) {
-                        const uint2 w = wv[u];
-                        iv[0] = w.x & 0xff;
-                        qv[0] = (w.x >> 8) & 0xff;
-                        iv[1] = (w.x >> 16) & 0xff;
-                        qv[1] = w.x >> 24;
-                        iv[2] = w.y & 0xff;
-                        qv[2] = (w.y >> 8) & 0xff;
-                        iv[3] = (w.y >> 16) & 0xff;
-                        qv[3] = w.y >> 24;
-                        f[0] = f[1] = f[2] = f[3] = true;
-                    } else {
-                        const uint8_t* rowp = a.raw + static_cast<long long>(y) * a.line_bytes;
-                        for (int k = 0; k < 4; ++k) {
-                            const int i = i0 + k;
-                            f[k] = (xb + k < a.nr) && (i >= 0) && (i < a.spl);
-                            iv[k] = qv[k] = 0;
-                            if (f[k]) {
-                                const uint16_t w = *reinterpret_cast<const uint16_t*>(rowp + 2ll * i);
-                                iv[k] = w & 0xff;
-                                qv[k] = w >> 8;
-                            }
-                        }
-                    }
-                    if (y >= y0) {
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            if (f[k]) {
-                                cnt += 1;
-                                si += iv[k];
-                                sq += qv[k];
-                                sii += iv[k] * iv[k];
-                                sqq += qv[k] * qv[k];
-                                siq += iv[k] * qv[k];
-                            }
-                            if (y > 0 && f[k] && pf[k]) {
-                                l[k][0] += 1;
-                                l[k][1] += pi[k];
-                                l[k][2] += pq[k];
-                                l[k][3] += iv[k];
-                                l[k][4] += qv[k];
-                                l[k][5] += pi[k] * iv[k];
-                                l[k][6] += pq[k] * qv[k];
-                                l[k][7] += pi[k] * qv[k];
-                                l[k][8] += pq[k] * iv[k];
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        pi[k] = iv[k];
-                        pq[k] = qv[k];
-                        pf[k] = f[k];
-                    }
-                }
-            }
+    const FastDiv dgpb = make_fastdiv(static_cast<unsigned int>(a.gpb));
+    for (int c = tid; c < kStatsCols; c += nthr) {
+        const int unit = bx * kStatsCols + c;
+        unsigned long long mv[6] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+        unsigned int lv[9] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        bool valid;
+        int blk;
+        if (a.quad) {
+            blk = static_cast<int>(fdiv_u(static_cast<unsigned int>(unit), dgpb));
+            const int x0 = blk * a.dc_step + 4 * (unit - blk * a.gpb);
+            const int xe = (blk + 1) * a.dc_step < a.nr ? (blk + 1) * a.dc_step : a.nr;
+            const int ncol = xe - x0 < 4 ? xe - x0 : 4;
+            valid = blk < a.nblk && ncol > 0;
+            if (valid) raw_stats_quad(a, sm, x0, ncol, y0, y1, ys, mv, lv);
+        } else {
+            valid = unit < a.nr;
+            blk = valid ? static_cast<int>(fdiv_u(static_cast<unsigned int>(unit), dstep)) : 0;
+            if (valid) raw_stats_column(a, sm, unit, y0, y1, ys, mv, lv);
         }
-        // the four columns belong to at most two Doppler blocks (blocks are >= 4 columns wide)
-        const int b_first = xin ? static_cast<int>(fdiv_u(xb, dstep)) : 0;
-        unsigned int la[9], lb[9];
-        int b_second = b_first;
-        for (int q = 0; q < 9; ++q) la[q] = lb[q] = 0u;
-        for (int k = 0; k < 4; ++k) {
-            const int x = xb + k;
-            if (!xin || x >= a.nr) continue;
-            const int bk = static_cast<int>(fdiv_u(x, dstep));
-            if (bk == b_first) {
-                for (int q = 0; q < 9; ++q) la[q] += l[k][q];
-            } else {
-                b_second = bk;
-                for (int q = 0; q < 9; ++q) lb[q] += l[k][q];
-            }
-        }
-        unsigned long long mv[6] = {cnt, si, sq, sii, sqq, siq};
-#if defined(__CUDA_ARCH__)
-        // warp reductions first: all lanes run this loop iteration (cols is a multiple of 4*nthr)
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            unsigned long long v = mv[k];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            mv[k] = v;
-        }
-        if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
-        }
-        const bool single = !xin || b_second == b_first;
-        const int bmin = __reduce_min_sync(0xffffffffu, xin ? b_first : 0x7fffffff);
-        const int bmax = __reduce_max_sync(0xffffffffu, xin ? b_first : -1);
-        const bool uniform = __all_sync(0xffffffffu, single) && bmin == bmax;
-        if (uniform) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) la[q] = __reduce_add_sync(0xffffffffu, xin ? la[q] : 0u);
-            if ((threadIdx.x & 31) == 0)
-                for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[bmin][q], la[q]);
-        } else if (xin) {
-            for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_first][q], la[q]);
-            if (b_second != b_first)
-                for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_second][q], lb[q]);
-        }
-#else
-        for (int k = 0; k < 6; ++k) atomic_add_u64(&sm->mom[k], mv[k]);
-        if (xin) {
-            for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_first][q], la[q]);
-            if (b_second != b_first)
-                for (int q = 0; q < 9; ++q) atomic_add_u64(&sm->lag[b_second][q], lb[q]);
-        }
-#endif
+        raw_stats_reduce(sm, valid, blk, mv, lv);
     }
     ASARF_SYNC();
     unsigned long long* gflat = &a.acc->mom[0];

@@ -22,11 +22,10 @@ struct TileBuf {
 };
 }  // namespace
 
-int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, int threads, int cols, void*) {
-    (void)threads;
+int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, void*) {
     RawStatsSmem sm;
     for (int by = 0; by < gy; ++by)
-        for (int bx = 0; bx < gx; ++bx) raw_stats_body(a, bx, by, 0, 1, cols, &sm);
+        for (int bx = 0; bx < gx; ++bx) raw_stats_body(a, bx, by, 0, 1, &sm);
     return ASARF_OK;
 }
 
@@ -188,10 +187,10 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
     st.min_swst = min_swst;
     st.dc_step = dc_step;
     st.nblk = nblk;
-    st.lines_per_cta = 64;
-    st.vec_ok = (reinterpret_cast<uintptr_t>(d_raw) % 8 == 0) && (raw_line_bytes % 8 == 0) ? 1 : 0;
+    st.lines_per_cta = kStatsMaxLines / 4;
     st.acc = &g_emu_scratch.acc;
-    backend_raw_stats(st, (range_size + 1023) / 1024, (azimuth_size + 63) / 64, 256, 1024, nullptr);
+    backend_raw_stats(st, raw_stats_grid_x(st, d_raw), (azimuth_size + st.lines_per_cta - 1) / st.lines_per_cta,
+                      nullptr);
     FinalizeArgs fin{};
     fin.acc = &g_emu_scratch.acc;
     fin.state = &g_emu_scratch.state;

@@ -393,7 +393,7 @@ struct asarf_plan {
     AzStridedArgs a_fwd{}, a_inv{};
     AzRdArgs a_rd{};
     TailArgs a_tail{};
-    int stats_gx = 0, stats_gy = 0, stats_cols = 256;
+    int stats_gy = 0;
     LaunchShape sh_rc{}, sh_st{}, sh_rd{}, sh_tail{};
     int tiles1 = 0, tiles2 = 0;
     int out_rows_max = 0, out_cols_max = 0;
@@ -693,10 +693,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     st.nr = p->nr;
     st.dc_step = dc_step;
     st.nblk = nblk;
-    st.lines_per_cta = 64;
+    st.lines_per_cta = kStatsMaxLines / 4;
     st.acc = p->acc;
-    p->stats_cols = 1024;  // 4 columns per thread, 256 threads
-    p->stats_gx = (p->nr + p->stats_cols - 1) / p->stats_cols;
     p->stats_gy = (p->na + st.lines_per_cta - 1) / st.lines_per_cta;
 
 
@@ -895,9 +893,9 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     st.raw = d_raw;
     st.swst = d_swst;
     st.min_swst = min_swst;
-    st.vec_ok = (reinterpret_cast<uintptr_t>(d_raw) % 8 == 0) && (p->scene.raw_line_bytes % 8 == 0) ? 1 : 0;
     mark();
-    rc = backend_raw_stats(st, p->stats_gx, p->stats_gy, 256, p->stats_cols, stream);
+    const int stats_gx = raw_stats_grid_x(st, d_raw);
+    rc = backend_raw_stats(st, stats_gx, p->stats_gy, stream);
     if (rc) return rc;
     mark();
     rc = backend_finalize(p->a_fin, stream);

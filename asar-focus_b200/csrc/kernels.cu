@@ -16,9 +16,9 @@ namespace asarf {
 
 namespace {
 
-__global__ void __launch_bounds__(256) k_raw_stats(RawStatsArgs a, int cols) {
+__global__ void __launch_bounds__(kStatsCols, 3) k_raw_stats(RawStatsArgs a) {
     __shared__ RawStatsSmem sm;
-    raw_stats_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cols, &sm);
+    raw_stats_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, &sm);
 }
 
 __global__ void k_finalize(FinalizeArgs a) {
@@ -173,8 +173,8 @@ cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 
 }  // namespace
 
-int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, int threads, int cols, void* stream) {
-    k_raw_stats<<<dim3(gx, gy), threads, 0, S(stream)>>>(a, cols);
+int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, void* stream) {
+    k_raw_stats<<<dim3(gx, gy), kStatsCols, 0, S(stream)>>>(a);
     return check_launch("raw_stats");
 }
 

@@ -59,9 +59,9 @@ int scratch_address(NoallocScratch** out) {
     return ASARF_OK;
 }
 
-__global__ void __launch_bounds__(256) k_noalloc_raw_stats(RawStatsArgs a, int cols) {
+__global__ void __launch_bounds__(kStatsCols) k_noalloc_raw_stats(RawStatsArgs a) {
     __shared__ RawStatsSmem sm;
-    raw_stats_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cols, &sm);
+    raw_stats_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, &sm);
 }
 
 __global__ void k_noalloc_finalize(FinalizeArgs a, asarf_raw_stats* out) {
@@ -129,12 +129,10 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
     st.min_swst = min_swst;
     st.dc_step = dc_step;
     st.nblk = nblk;
-    st.lines_per_cta = 64;
-    st.vec_ok = (reinterpret_cast<uintptr_t>(d_raw) % 8 == 0) && (raw_line_bytes % 8 == 0) ? 1 : 0;
+    st.lines_per_cta = kStatsMaxLines / 4;
     st.acc = &scratch->acc;
-    const int cols = 1024;
-    dim3 grid((range_size + cols - 1) / cols, (azimuth_size + st.lines_per_cta - 1) / st.lines_per_cta);
-    k_noalloc_raw_stats<<<grid, 256, 0, s>>>(st, cols);
+    dim3 grid(raw_stats_grid_x(st, d_raw), (azimuth_size + st.lines_per_cta - 1) / st.lines_per_cta);
+    k_noalloc_raw_stats<<<grid, kStatsCols, 0, s>>>(st);
 
     FinalizeArgs fin{};
     fin.acc = &scratch->acc;

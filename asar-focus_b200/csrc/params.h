@@ -71,8 +71,9 @@ struct RawStatsArgs {
     const uint16_t* swst; // nullable
     int min_swst;
     int dc_step, nblk;
-    int lines_per_cta;
-    int vec_ok;           // raw base and line stride 8-byte aligned: 4 samples per load
+    int lines_per_cta;    // at most kStatsMaxLines
+    int quad;             // 4-column units (raw base and line stride 8-byte aligned)
+    int gpb;              // 4-column groups per Doppler block: ceil(dc_step / 4)
     StatAccum* acc;
 };
 
