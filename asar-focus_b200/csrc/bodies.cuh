@@ -577,8 +577,20 @@ ASARF_HD ASARF_INLINE void range_compress_ct_body(const RangeCompressArgs& a, in
 // write the digit-reversed transform output straight to its destination rows.
 // Together with the contiguous pass this is the transpose-free equivalent of the reference's
 // transpose + batched row FFT + transpose (sar/range_doppler_algorithm.cu:314-326, 381-391).
+// Per-block tables of the strided pass, staged in shared memory while the tile is in flight:
+// tw[p] = W_N^{b * k1} and row[p] = destination row, for transform position p (forward:
+// k1 = drev1(p), digit-reversed output; inverse: tw indexed by the natural input row k1 = p,
+// row by the digit-reversed output position).  b * k1 < N, so no reduction is needed.
+ASARF_HD ASARF_INLINE void az_strided_tables(const AzStridedArgs& a, int b, int tid, int nthr, float2* tw, int* row) {
+    for (int p = tid; p < a.n1; p += nthr) {
+        const int kd = ASARF_LDG(a.drev1 + p);
+        tw[p] = ASARF_LDG(a.twn + b * (a.inverse ? p : kd));
+        row[p] = kd * a.n2 + b;
+    }
+}
+
 ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int b, int tid, int nthr, float2* s,
-                                           bool preloaded) {
+                                           const float2* tw, const int* rowmap, bool preloaded) {
     const int x0 = tile * a.xt;
     const int n1 = a.n1, xt = a.xt;
     const FastDiv dxt = make_fastdiv(static_cast<unsigned int>(xt));
@@ -602,17 +614,13 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
         fft_forward_pairs(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
-            const int k1 = ASARF_LDG(a.drev1 + p);
             const int x = x0 + c;
-            if (x < a.nk) {
-                const float2 tw = ASARF_LDG(a.twn + b * k1);
-                a.out[static_cast<long long>(k1 * a.n2 + b) * a.pitch + x] = cmul(s[t], tw);
-            }
+            if (x < a.nk) a.out[static_cast<long long>(rowmap[p]) * a.pitch + x] = cmul(s[t], tw[p]);
         }
     } else {
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int k1 = static_cast<int>(fdiv_u(t, dxt));
-            s[t] = cmulc(s[t], ASARF_LDG(a.twn + b * k1));
+            s[t] = cmulc(s[t], tw[k1]);
         }
         ASARF_SYNC();
         fft_inverse_dif_pairs(a.plan1, s, xt, xt, tid, nthr);
@@ -620,7 +628,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
-            const int row = ASARF_LDG(a.drev1 + p) * a.n2 + b;
+            const int row = rowmap[p];
             const int x = x0 + c;
             if (x < a.nk && row >= lo && row < hi) {
                 const float2 v = s[t];
@@ -628,6 +636,11 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
             }
         }
     }
+}
+
+// Shared-memory bytes of the strided pass: tile, twiddle table, row table.
+inline size_t az_strided_smem(int n1, int xt) {
+    return sizeof(float2) * static_cast<size_t>(n1) * xt + sizeof(float2) * n1 + sizeof(int) * n1;
 }
 
 // ----------------------------------------------------------------------------- range-Doppler block

@@ -58,8 +58,12 @@ int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh
 
 int backend_az_strided(const AzStridedArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, void*) {
     TileBuf s(sh.smem);
-    for (int b = 0; b < nblocks; ++b)
-        for (int t = 0; t < tiles; ++t) az_strided_body(a, t, b, 0, 1, s.data(), false);
+    float2* tw = s.data() + static_cast<size_t>(a.n1) * a.xt;
+    int* row = reinterpret_cast<int*>(tw + a.n1);
+    for (int b = 0; b < nblocks; ++b) {
+        az_strided_tables(a, b, 0, 1, tw, row);
+        for (int t = 0; t < tiles; ++t) az_strided_body(a, t, b, 0, 1, s.data(), tw, row, false);
+    }
     return ASARF_OK;
 }
 

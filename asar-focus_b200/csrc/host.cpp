@@ -757,7 +757,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     p->a_inv.scale = 1.0f / static_cast<float>(p->az_pad);
     p->a_inv.inverse = 1;
     p->tiles1 = (p->nk + p->xt1 - 1) / p->xt1;
-    p->sh_st = {256, sizeof(float2) * static_cast<size_t>(p->n1) * p->xt1};
+    p->sh_st = {256, az_strided_smem(p->n1, p->xt1)};
 
     AzRdArgs& d = p->a_rd;
     d.in = p->bufA;

@@ -77,18 +77,20 @@ __global__ void __launch_bounds__(CtSchedule<L>::nthr, 2) k_range_compress_ct(Ra
 __global__ void __launch_bounds__(512) k_az_strided(AzStridedArgs a, const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(1024) unsigned char smem_as_raw[];
     float2* s = reinterpret_cast<float2*>(smem_as_raw);
+    float2* tw = s + static_cast<size_t>(a.n1) * a.xt;
+    int* row = reinterpret_cast<int*>(tw + a.n1);
     __shared__ uint64_t bar;
-    if (a.use_tma) {
-        if (threadIdx.x == 0) {
-            mbar_init(&bar, 1);
-            mbar_expect_tx(&bar, static_cast<uint32_t>(sizeof(float2) * a.n1 * a.xt));
-            for (int r0 = 0; r0 < a.n1; r0 += a.n1_box)
-                tma_load_3d(s + static_cast<size_t>(r0) * a.xt, &map, &bar, 2 * blockIdx.x * a.xt, blockIdx.y, r0);
-        }
-        __syncthreads();
-        mbar_wait(&bar, 0, a.state ? &const_cast<FocusState*>(a.state)->errors : nullptr);
+    if (a.use_tma && threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, static_cast<uint32_t>(sizeof(float2) * a.n1 * a.xt));
+        for (int r0 = 0; r0 < a.n1; r0 += a.n1_box)
+            tma_load_3d(s + static_cast<size_t>(r0) * a.xt, &map, &bar, 2 * blockIdx.x * a.xt, blockIdx.y, r0);
     }
-    az_strided_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, a.use_tma != 0);
+    // twiddle and row tables are gathered while the tile is in flight
+    az_strided_tables(a, blockIdx.y, threadIdx.x, blockDim.x, tw, row);
+    __syncthreads();
+    if (a.use_tma) mbar_wait(&bar, 0, a.state ? &const_cast<FocusState*>(a.state)->errors : nullptr);
+    az_strided_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, tw, row, a.use_tma != 0);
 }
 
 // Range-Doppler block: the [n2][wt] tile (contiguous rows, range halo) arrives by 2-D TMA
