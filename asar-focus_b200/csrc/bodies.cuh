@@ -753,13 +753,27 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
     return cmul(out, expj_neg_sum(mf_phase, sh_phase));
 }
 
-ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s, float2* tmp,
-                                      ColParams* cps, unsigned int* err_flag, bool preloaded) {
+// Per-block tables of the range-Doppler block, built while the tile is in flight: column
+// constants of the xt output columns and the frequency bin of each of the n2 rows.
+ASARF_HD ASARF_INLINE void az_rd_tables(const AzRdArgs& a, int tile, int k1, int tid, int nthr, ColParams* cps,
+                                        int* fbin) {
+    const int x0 = tile * a.xt;
+    for (int c = tid; c < a.xt; c += nthr) cps[c] = az_col_params(a, x0 + c);
+    for (int p = tid; p < a.n2; p += nthr) fbin[p] = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
+}
+
+// Shared-memory bytes of the range-Doppler block: tile, column constants, row bins.
+inline size_t az_rd_smem(int n2, int wt, int xt) {
+    return sizeof(float2) * static_cast<size_t>(n2) * wt + sizeof(ColParams) * static_cast<size_t>(xt) +
+           sizeof(int) * static_cast<size_t>(n2) + 16;
+}
+
+ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s,
+                                      const ColParams* cps, const int* fbin, unsigned int* err_flag, bool preloaded) {
     const int x0 = tile * a.xt;
     const int n2 = a.n2, wt = a.wt;
     const FastDiv dwt = make_fastdiv(static_cast<unsigned int>(wt));
     const FastDiv dxt = make_fastdiv(static_cast<unsigned int>(a.xt));
-    (void)dxt;
     if (!preloaded) {
         for (int t = tid; t < n2 * wt; t += nthr) {
             const int r = static_cast<int>(fdiv_u(t, dwt)), c = t - r * wt;
@@ -769,7 +783,6 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
             s[t] = v;
         }
     }
-    for (int c = tid; c < a.xt; c += nthr) cps[c] = az_col_params(a, x0 + c);
     ASARF_SYNC();
     fft_forward_pairs(a.plan2, s, wt, wt, tid, nthr);
     // RCMC + matched filter.  Every output (row p, column c) reads taps of row p only, so a
@@ -779,7 +792,7 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     {
         const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
         for (int p = warp; p < n2; p += nwarps) {
-            const int f = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
+            const int f = fbin[p];
             const float2* srow = s + p * wt;
             float2 v0 = make_float2(0.0f, 0.0f), v1 = make_float2(0.0f, 0.0f);
             const int c0 = lane, c1 = lane + 32;
@@ -796,13 +809,12 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     {
         float2 rowbuf[64];
         for (int p = 0; p < n2; ++p) {
-            const int f = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
+            const int f = fbin[p];
             for (int c = 0; c < a.xt; ++c)
                 rowbuf[c] = (x0 + c < a.nk) ? rcmc_mf_sample(a, cps[c], x0 + c, f, s + p * wt, a.hl + c, err_flag)
                                             : make_float2(0.0f, 0.0f);
             for (int c = 0; c < a.xt; ++c) s[p * wt + a.hl + c] = rowbuf[c];
         }
-        (void)tmp;
     }
 #endif
     fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr);

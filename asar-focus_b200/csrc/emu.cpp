@@ -70,10 +70,13 @@ int backend_az_strided(const AzStridedArgs& a, const void*, int tiles, int nbloc
 int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void*) {
     TileBuf buf(sh.smem + 128);
     float2* s = buf.data();
-    float2* tmp = s + a.n2 * a.wt;
-    ColParams* cps = reinterpret_cast<ColParams*>(tmp);
+    ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * a.wt);
+    int* fbin = reinterpret_cast<int*>(cps + a.xt);
     for (int b = 0; b < nblocks; ++b)
-        for (int t = 0; t < tiles; ++t) az_rd_body(a, t, b, 0, 1, s, tmp, cps, err, false);
+        for (int t = 0; t < tiles; ++t) {
+            az_rd_tables(a, t, b, 0, 1, cps, fbin);
+            az_rd_body(a, t, b, 0, 1, s, cps, fbin, err, false);
+        }
     return ASARF_OK;
 }
 

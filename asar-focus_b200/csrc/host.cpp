@@ -785,7 +785,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     d.state = p->state;
     d.win = win;
     p->tiles2 = (p->nk + p->xt2 - 1) / p->xt2;
-    p->sh_rd = {512, sizeof(float2) * static_cast<size_t>(p->n2) * d.wt + sizeof(ColParams) * d.xt + 16};
+    p->sh_rd = {512, az_rd_smem(p->n2, d.wt, d.xt)};
 
     TailArgs& t = p->a_tail;
     t.slc = p->bufB;

@@ -99,21 +99,21 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
     extern __shared__ __align__(1024) unsigned char smem_rd_raw[];
     const int wt = a.wt;
     float2* s = reinterpret_cast<float2*>(smem_rd_raw);
-    float2* tmp = s + a.n2 * wt;
-    ColParams* cps = reinterpret_cast<ColParams*>(tmp);
+    ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * wt);
+    int* fbin = reinterpret_cast<int*>(cps + a.xt);
     __shared__ uint64_t bar;
-    if (a.use_tma) {
-        if (threadIdx.x == 0) {
-            mbar_init(&bar, 1);
-            mbar_expect_tx(&bar, static_cast<uint32_t>(sizeof(float2) * a.n2 * wt));
-            const int x = 2 * (static_cast<int>(blockIdx.x) * a.xt - a.hl);
-            for (int r0 = 0; r0 < a.n2; r0 += a.n2_box)
-                tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
-        }
-        __syncthreads();
-        mbar_wait(&bar, 0, err);
+    if (a.use_tma && threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, static_cast<uint32_t>(sizeof(float2) * a.n2 * wt));
+        const int x = 2 * (static_cast<int>(blockIdx.x) * a.xt - a.hl);
+        for (int r0 = 0; r0 < a.n2; r0 += a.n2_box)
+            tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
     }
-    az_rd_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, tmp, cps, err, a.use_tma != 0);
+    // column constants and row bins are computed while the tile is in flight
+    az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbin);
+    __syncthreads();
+    if (a.use_tma) mbar_wait(&bar, 0, err);
+    az_rd_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, a.use_tma != 0);
 }
 
 __global__ void __launch_bounds__(512) k_tail(TailArgs a, unsigned int* err) {

@@ -308,7 +308,7 @@ int asarf_range_doppler(const asarf_rda_params* prm, void* d_src, void* d_out, i
     for (int k = 0; k < 3; ++k) d.vr_poly[k] = static_cast<float>(prm->vr_poly[k]);
     d.state = dstate;
     const LaunchShape sh_st{256, az_strided_smem(n1, xt1)};
-    const LaunchShape sh_rd{512, sizeof(float2) * static_cast<size_t>(n2) * d.wt + sizeof(ColParams) * d.xt + 16};
+    const LaunchShape sh_rd{512, az_rd_smem(n2, d.wt, d.xt)};
     if (sh_st.smem > smem_optin_limit() || sh_rd.smem > smem_optin_limit())
         return set_error(ASARF_ERR_INVALID, "range_doppler: tiles exceed shared memory (n1 %d, n2 %d)", n1, n2);
     const int tiles1 = (x_size + xt1 - 1) / xt1, tiles2 = (x_size + d.xt - 1) / d.xt;
