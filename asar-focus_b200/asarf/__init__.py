@@ -14,7 +14,8 @@ from . import _lib
 from ._lib import AsarfError, load_library
 from .scene import Scene
 
-__all__ = ["FocusPlan", "Scene", "AsarfError", "load_library", "version", "fft_size_above"]
+__all__ = ["FocusPlan", "FocusBatch", "Scene", "AsarfError", "load_library", "version", "fft_size_above",
+           "lpt_assign"]
 
 
 def version(lib=None) -> str:
@@ -62,7 +63,21 @@ class FocusPlan:
         self.dims = {f: (list(getattr(d, f)) if f in ("out_rows", "out_cols", "vr_poly") else getattr(d, f))
                      for f, _ in d._fields_}
 
+    @classmethod
+    def _wrap(cls, lib, handle, scene, owner):
+        """A view of a plan owned by someone else (a batch): never destroyed through this object."""
+        self = cls.__new__(cls)
+        self.lib, self.scene, self._h, self._owner = lib, scene, handle, owner
+        d = _lib.Dims()
+        _lib.check(lib, lib.asarf_plan_dims(handle, C.byref(d)), "plan_dims")
+        self.dims = {f: (list(getattr(d, f)) if f in ("out_rows", "out_cols", "vr_poly") else getattr(d, f))
+                     for f, _ in d._fields_}
+        return self
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             self.lib.asarf_plan_destroy(self._h)
             self._h = None
@@ -130,3 +145,68 @@ class FocusPlan:
         [n_lines, slc_cols], device memory or, for a host build, host memory)."""
         _lib.check(self.lib, self.lib.asarf_plan_slc(self._h, C.c_void_p(_ptr(dst)), C.c_void_p(stream)), "plan_slc")
         return dst
+
+
+def lpt_assign(work, bins: int, lib=None) -> list[int]:
+    """Longest-processing-time assignment of work items to bins (asarf_lpt_assign): the rule
+    that deals batch segments to graph branches and to GPUs."""
+    lib = lib or load_library()
+    n = len(work)
+    w = (C.c_int64 * n)(*[int(v) for v in work])
+    out = (C.c_int32 * max(n, 1))()
+    _lib.check(lib, lib.asarf_lpt_assign(w, n, int(bins), out), "lpt_assign")
+    return [int(out[i]) for i in range(n)]
+
+
+class FocusBatch:
+    """Independent segments of uneven size focused together (asarf_batch): every segment's
+    kernels in one CUDA graph with concurrent branches, replayed on later calls with the same
+    buffers.  ``plans[i]`` is segment i's plan (dims, results, SLC)."""
+
+    def __init__(self, scenes, branches: int = 4, ref_compat_stats: bool = True, lib=None, lib_path=None):
+        self.lib = lib or load_library(lib_path)
+        self.scenes = list(scenes)
+        n = len(self.scenes)
+        for sc in self.scenes:
+            if sc.vr_poly is None or not sc.osv:
+                sc.prepare(self.lib)
+        self._keep = [sc.to_c() for sc in self.scenes]
+        arr = (_lib.SceneC * n)(*[k[0] for k in self._keep])
+        opts = (_lib.Options * n)()
+        for i in range(n):
+            self.lib.asarf_default_options(C.byref(opts[i]))
+            opts[i].ref_compat_stats = int(bool(ref_compat_stats))
+        h = C.c_void_p()
+        _lib.check(self.lib, self.lib.asarf_batch_create(arr, n, C.cast(opts, C.c_void_p), int(branches), C.byref(h)),
+                   "batch_create")
+        self._h = h
+        self.plans = []
+        for i in range(n):
+            ph = C.c_void_p()
+            _lib.check(self.lib, self.lib.asarf_batch_plan(self._h, i, C.byref(ph)), "batch_plan")
+            self.plans.append(FocusPlan._wrap(self.lib, ph, self.scenes[i], self))
+        self.branches = [int(self.lib.asarf_batch_branch(self._h, i)) for i in range(n)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for p in self.plans:
+                p.close()
+            self.lib.asarf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def focus(self, raws, outs, swsts=None, min_swst=None, stream: int = 0):
+        """Asynchronous focus of every segment: raws[i] (device raw bytes) -> outs[i] (float32
+        [out_rows_max, out_cols_max] of plans[i])."""
+        n = len(self.plans)
+        r = (C.c_void_p * n)(*[_ptr(x) for x in raws])
+        o = (C.c_void_p * n)(*[_ptr(x) for x in outs])
+        sw = C.cast((C.c_void_p * n)(*[_ptr(x) for x in swsts]), C.c_void_p) if swsts is not None else None
+        mn = C.cast((C.c_int32 * n)(*[int(v) for v in min_swst]), C.c_void_p) if min_swst is not None else None
+        _lib.check(self.lib, self.lib.asarf_batch_focus(self._h, r, sw, mn, o, C.c_void_p(stream)), "batch_focus")
+        return outs

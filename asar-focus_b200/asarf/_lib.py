@@ -106,6 +106,13 @@ _SIGS = {
     "asarf_raw_statistics_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                                C.c_int32, C.c_int64, C.c_int32, C.c_double, C.c_void_p,
                                                C.c_void_p]),
+    "asarf_batch_create": (C.c_int, [C.POINTER(SceneC), C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "asarf_batch_destroy": (None, [C.c_void_p]),
+    "asarf_batch_plan": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "asarf_batch_branch": (C.c_int, [C.c_void_p, C.c_int32]),
+    "asarf_batch_focus": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_void_p), C.c_void_p]),
+    "asarf_lpt_assign": (C.c_int, [C.POINTER(C.c_int64), C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     # per-stage entry points
     "asarf_convert_ers_samples": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
                                             C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),

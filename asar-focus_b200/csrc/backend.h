@@ -47,6 +47,16 @@ void event_destroy(void* e);
 int event_record(void* e, void* stream);
 int event_elapsed(void* a, void* b, float* ms);
 size_t smem_optin_limit();
+// Streams, cross-stream waits and CUDA graphs (device build).  The host emulation has no
+// graphs: graphs_supported() is false there and callers run their sequence directly.
+void* stream_create();
+void stream_destroy(void* s);
+int stream_wait_event(void* stream, void* event);
+bool graphs_supported();
+int graph_capture_begin(void* stream);
+int graph_capture_end(void* stream, void** exec);
+int graph_launch(void* exec, void* stream);
+void graph_destroy(void* exec);
 const char* backend_name();
 // Encode a float32 tiled tensor map (128-byte blob) of `rank` dims: dims[rank] innermost
 // first, strides[rank-1] in bytes, box[rank]; zero fill out of bounds.

@@ -231,6 +231,14 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
 }
 
 namespace asarf {
+void* stream_create() { return std::calloc(1, 8); }
+void stream_destroy(void* s) { std::free(s); }
+int stream_wait_event(void*, void*) { return ASARF_OK; }
+bool graphs_supported() { return false; }
+int graph_capture_begin(void*) { return set_error(ASARF_ERR_INVALID, "no graphs in the host emulation"); }
+int graph_capture_end(void*, void**) { return set_error(ASARF_ERR_INVALID, "no graphs in the host emulation"); }
+int graph_launch(void*, void*) { return set_error(ASARF_ERR_INVALID, "no graphs in the host emulation"); }
+void graph_destroy(void*) {}
 const char* backend_name() { return "host-emulation"; }
 int backend_make_tmap(void*, int, void*, const unsigned long long*, const unsigned long long*, const unsigned int*) {
     return set_error(ASARF_ERR_INVALID, "no tensor maps in host emulation");

@@ -365,6 +365,42 @@ int event_elapsed(void* a, void* b, float* ms) {
     return cuda_rc(e, "event elapsed");
 }
 
+void* stream_create() {
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return s;
+}
+void stream_destroy(void* s) {
+    if (s) cudaStreamDestroy(static_cast<cudaStream_t>(s));
+}
+int stream_wait_event(void* stream, void* event) {
+    return cuda_rc(cudaStreamWaitEvent(S(stream), static_cast<cudaEvent_t>(event), 0), "stream wait");
+}
+bool graphs_supported() { return true; }
+int graph_capture_begin(void* stream) {
+    return cuda_rc(cudaStreamBeginCapture(S(stream), cudaStreamCaptureModeRelaxed), "begin capture");
+}
+int graph_capture_end(void* stream, void** exec) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(S(stream), &g);
+    if (e != cudaSuccess) return cuda_rc(e, "end capture");
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_rc(e, "graph instantiate");
+    *exec = x;
+    return ASARF_OK;
+}
+int graph_launch(void* exec, void* stream) {
+    return cuda_rc(cudaGraphLaunch(static_cast<cudaGraphExec_t>(exec), S(stream)), "graph launch");
+}
+void graph_destroy(void* exec) {
+    if (exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(exec));
+}
+
 size_t smem_optin_limit() {
     int dev = 0, v = 0;
     cudaGetDevice(&dev);

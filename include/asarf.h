@@ -202,6 +202,32 @@ int asarf_srgr_polynomial(const asarf_scene* scene, double slant_first, int32_t 
 int32_t asarf_fft_size_above(int32_t v);
 
 /* ---------------------------------------------------------------------------------------
+ * Batches of independent segments of uneven size.  No reference counterpart: the reference
+ * focuses one scene per process run (main.cc:176-327).  Each segment gets its own plan;
+ * asarf_batch_focus captures every segment's kernels once into a CUDA graph whose branches
+ * (up to `branches` side streams, segments dealt largest first) run concurrently, and
+ * replays it on later calls with the same buffers (new buffers: a new capture; the first
+ * call with a set of buffers also runs the segments once directly, outside the capture).
+ * ------------------------------------------------------------------------------------- */
+typedef struct asarf_batch asarf_batch;
+
+/* opts: NULL or one asarf_options per scene; branches <= 0 means 4. */
+int asarf_batch_create(const asarf_scene* scenes, int32_t n, const asarf_options* opts, int32_t branches,
+                       asarf_batch** out);
+void asarf_batch_destroy(asarf_batch* batch);
+/* The plan of segment i (owned by the batch): dims, results, SLC access. */
+int asarf_batch_plan(asarf_batch* batch, int32_t i, asarf_plan** out);
+/* Branch (side stream index) segment i runs on, -1 if i is out of range. */
+int asarf_batch_branch(const asarf_batch* batch, int32_t i);
+/* Segment i: raw bytes d_raw[i], SWST codes d_swst[i] (d_swst may be NULL, or hold NULLs),
+ * min_swst[i] (NULL = 0), detected output d_out[i] (asarf_focus's layout). */
+int asarf_batch_focus(asarf_batch* batch, const uint8_t* const* d_raw, const uint16_t* const* d_swst,
+                      const int32_t* min_swst, float* const* d_out, void* stream);
+/* Longest-processing-time assignment of n work items to `bins` bins (largest item first,
+ * to the least-loaded bin): the rule that deals segments to graph branches and to GPUs. */
+int asarf_lpt_assign(const int64_t* work, int32_t n, int32_t bins, int32_t* out_bin);
+
+/* ---------------------------------------------------------------------------------------
  * Per-stage entry points: the reference's sar/ functions one at a time, for a caller that
  * keeps the reference's own pipeline (main.cc) and swaps stages.  Images use the layout of
  * DevicePaddedImage (cuda_util/device_padded_image.cuh:13-27): complex float
