@@ -14,7 +14,7 @@ from . import _lib
 from ._lib import AsarfError, load_library
 from .scene import Scene
 
-__all__ = ["FocusPlan", "FocusBatch", "Scene", "AsarfError", "load_library", "version", "fft_size_above",
+__all__ = ["FocusPlan", "FocusBatch", "FocusStrip", "Scene", "AsarfError", "load_library", "version", "fft_size_above",
            "lpt_assign"]
 
 
@@ -210,3 +210,66 @@ class FocusBatch:
         mn = C.cast((C.c_int32 * n)(*[int(v) for v in min_swst]), C.c_void_p) if min_swst is not None else None
         _lib.check(self.lib, self.lib.asarf_batch_focus(self._h, r, sw, mn, o, C.c_void_p(stream)), "batch_focus")
         return outs
+
+
+class FocusStrip:
+    """A long strip focused as overlapped azimuth blocks (asarf_strip): per-block statistics,
+    Doppler estimate and Vr, one strip SLC, one multilook/RSL/SRGR pass over the strip."""
+
+    def __init__(self, scene: Scene, block_lines: int = 16384, overlap: int = 1400, ref_compat_stats: bool = True,
+                 lib=None, lib_path=None):
+        self.lib = lib or load_library(lib_path)
+        self.scene = scene
+        if scene.vr_poly is None or not scene.osv:
+            scene.prepare(self.lib)
+        self._sc, self._osv_keep = scene.to_c()
+        opt = _lib.Options()
+        self.lib.asarf_default_options(C.byref(opt))
+        opt.ref_compat_stats = int(bool(ref_compat_stats))
+        self._opt = opt
+        h = C.c_void_p()
+        _lib.check(self.lib, self.lib.asarf_strip_create(C.byref(self._sc), int(block_lines), int(overlap),
+                                                         C.cast(C.byref(opt), C.c_void_p), C.byref(h)), "strip_create")
+        self._h = h
+        d = _lib.StripDims()
+        _lib.check(self.lib, self.lib.asarf_strip_get_dims(self._h, C.byref(d)), "strip_dims")
+        self.dims = {f: getattr(d, f) for f, _ in d._fields_}
+        self.blocks = []
+        for k in range(self.dims["n_blocks"]):
+            s0, lo, hi, ph = C.c_int32(), C.c_int32(), C.c_int32(), C.c_void_p()
+            _lib.check(self.lib, self.lib.asarf_strip_block(self._h, k, C.byref(s0), C.byref(lo), C.byref(hi),
+                                                            C.byref(ph)), "strip_block")
+            self.blocks.append({"start": s0.value, "keep_lo": lo.value, "keep_hi": hi.value,
+                                "plan": FocusPlan._wrap(self.lib, ph, scene, self)})
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for b in self.blocks:
+                b["plan"].close()
+            self.lib.asarf_strip_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def out_shape(self) -> tuple[int, int]:
+        return self.dims["out_rows"], self.dims["out_cols"]
+
+    def focus(self, raw, out, swst=None, min_swst: int = 0, stream: int = 0):
+        _lib.check(self.lib, self.lib.asarf_focus_strip(self._h, _ptr(raw), _ptr(swst), int(min_swst), _ptr(out),
+                                                        C.c_void_p(stream)), "focus_strip")
+        return out
+
+    def slc_into(self, dst, stream: int = 0):
+        """Strip SLC, complex64 [slc_rows, slc_cols]."""
+        _lib.check(self.lib, self.lib.asarf_strip_slc(self._h, C.c_void_p(_ptr(dst)), C.c_void_p(stream)), "strip_slc")
+        return dst
+
+    def errors(self, stream: int = 0) -> int:
+        e = C.c_uint32()
+        _lib.check(self.lib, self.lib.asarf_strip_errors(self._h, C.byref(e), C.c_void_p(stream)), "strip_errors")
+        return int(e.value)

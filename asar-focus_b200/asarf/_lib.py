@@ -75,6 +75,13 @@ class RdaParams(C.Structure):
                 ("dc_poly", C.c_double * 3)]
 
 
+class StripDims(C.Structure):
+    _fields_ = [("n_blocks", C.c_int32), ("block_lines", C.c_int32), ("overlap", C.c_int32),
+                ("first_line", C.c_int32), ("slc_rows", C.c_int32), ("slc_cols", C.c_int32),
+                ("slc_pitch", C.c_int32), ("out_rows", C.c_int32), ("out_cols", C.c_int32),
+                ("max_aperture", C.c_int32), ("device_bytes", C.c_size_t)]
+
+
 class AsarfError(RuntimeError):
     pass
 
@@ -113,6 +120,14 @@ _SIGS = {
     "asarf_batch_focus": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p,
                                     C.POINTER(C.c_void_p), C.c_void_p]),
     "asarf_lpt_assign": (C.c_int, [C.POINTER(C.c_int64), C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "asarf_strip_create": (C.c_int, [C.POINTER(SceneC), C.c_int32, C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "asarf_strip_destroy": (None, [C.c_void_p]),
+    "asarf_strip_get_dims": (C.c_int, [C.c_void_p, C.POINTER(StripDims)]),
+    "asarf_strip_block": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int32), C.POINTER(C.c_void_p)]),
+    "asarf_focus_strip": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "asarf_strip_slc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "asarf_strip_errors": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]),
     # per-stage entry points
     "asarf_convert_ers_samples": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
                                             C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),

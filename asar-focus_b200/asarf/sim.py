@@ -88,6 +88,14 @@ def simulate(sc: Scene, device: str | torch.device = "cpu", noise_rel: float = 0
         spec[:, c0:c1] *= h.to(cdt)
     clut = torch.fft.ifft(spec, dim=0)
     del spec
+    if sc.dc_kind == "sin" and sc.dc_drift:
+        # azimuth drift of the clutter's Doppler centroid: line y is shifted in frequency by
+        # dc_truth(y) - dc_truth(mid-scene) through the integrated phase of that shift
+        yy = np.arange(na, dtype=np.float64)
+        shift = sc.dc_drift * np.sin(2 * np.pi * yy / na) - sc.dc_drift * np.sin(np.pi)
+        phase = 2 * np.pi * np.cumsum(shift) / prf
+        clut = clut * torch.polar(torch.ones(na, device=dev, dtype=torch.float64),
+                                  torch.as_tensor(np.remainder(phase, 2 * np.pi), device=dev))[:, None].to(cdt)
     clut_std = float(torch.sqrt(torch.mean(clut.real ** 2 + clut.imag ** 2) / 2))
 
     # ---------------------------------------------------------------- point targets

@@ -632,7 +632,8 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
             const int x = x0 + c;
             if (x < a.nk && row >= lo && row < hi) {
                 const float2 v = s[t];
-                a.out[static_cast<long long>(row) * a.pitch + x] = make_float2(fmul_rn(v.x, a.scale), fmul_rn(v.y, a.scale));
+                a.out[static_cast<long long>(row - a.out_row0) * a.pitch + x] =
+                    make_float2(fmul_rn(v.x, a.scale), fmul_rn(v.y, a.scale));
             }
         }
     }

@@ -13,6 +13,7 @@
 #include "backend.h"
 #include "bodies.cuh"
 #include "internal.h"
+#include "plan.h"
 
 namespace asarf {
 
@@ -130,7 +131,7 @@ static int aperture_pixels_at(const asarf_scene& s, const double* vr_poly, int p
     return static_cast<int>(round_half_away((fmax / ka) * s.prf));
 }
 
-static int max_aperture_pixels(const asarf_scene& s) {
+int max_aperture_pixels(const asarf_scene& s) {
     // CalcAperturePixels(sar_meta) (sar/sar_metadata.h:126-141) as main.cc:251 calls it
     const int range_end = s.range_size - s.chirp_samples;
     const int step = range_end / 10;
@@ -180,7 +181,7 @@ static int estimate_vr_poly(const asarf_scene& s, double out[3]) {
     return ASARF_OK;
 }
 
-static int srgr_poly(const asarf_scene& s, double slant_first, int range_size, int azimuth_size, double lti,
+int srgr_poly(const asarf_scene& s, double slant_first, int range_size, int azimuth_size, double lti,
                      double poly[5], int* ng) {
     // SlantRangeToGroundRangeInterpolation setup (sar/srgr.cu:73-121)
     const int N = 100;
@@ -364,63 +365,6 @@ int choose_rc_len(int nr) {
 
 using namespace asarf;
 
-struct asarf_plan {
-    asarf_scene scene{};
-    std::vector<asarf_osv> osv;
-    asarf_options opt{};
-    asarf_dims dims{};
-    int nr = 0, na = 0, nc = 0, nk = 0, nx = 0;
-    int rg_pad_ref = 0, az_pad = 0, rc_len = 0, n1 = 0, n2 = 0;
-    long long pitch = 0;
-    int xt1 = 32, xt2 = 32, hl = 8, hr = 8;
-    double vr_poly[3] = {0, 0, 0};
-    // device memory
-    std::vector<void*> allocs;
-    size_t bytes = 0;
-    float2* bufA = nullptr;
-    float2* bufB = nullptr;
-    StatAccum* acc = nullptr;
-    FocusState* state = nullptr;
-    uint8_t* raw_dev = nullptr;
-    uint16_t* swst_dev = nullptr;
-    float* out_dev = nullptr;
-    HostFft rc, f1, f2, fN;
-    float2* rc_mf = nullptr;
-    // launch argument blocks
-    RawStatsArgs a_stats{};
-    FinalizeArgs a_fin{};
-    RangeCompressArgs a_rc{};
-    AzStridedArgs a_fwd{}, a_inv{};
-    AzRdArgs a_rd{};
-    TailArgs a_tail{};
-    int stats_gy = 0;
-    LaunchShape sh_rc{}, sh_st{}, sh_rd{}, sh_tail{};
-    int tiles1 = 0, tiles2 = 0;
-    int out_rows_max = 0, out_cols_max = 0;
-    // optional per-kernel timing (events recorded between the launches of each run)
-    std::vector<void*> events;
-    int timing_slots = 0, timing_used = 0;
-    // TMA tensor maps (device build): strided views of A and B, contiguous view of A
-    alignas(64) unsigned char tmapA3[128] = {};
-    alignas(64) unsigned char tmapB3[128] = {};
-    alignas(64) unsigned char tmapA2[128] = {};
-    bool use_tma = false;
-    int raw_smem_offset = 0;
-
-    template <class T>
-    T* alloc(size_t count) {
-        void* p = mem_alloc(count * sizeof(T));
-        if (p) {
-            allocs.push_back(p);
-            bytes += count * sizeof(T);
-        }
-        return static_cast<T*>(p);
-    }
-    ~asarf_plan() {
-        for (void* e : events) event_destroy(e);
-        for (void* p : allocs) mem_free(p);
-    }
-};
 
 extern "C" {
 
@@ -875,7 +819,7 @@ static const char* const kKernelNames[kKernelsPerRun] = {"raw_stats", "finalize"
 
 int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int32_t min_swst, float* d_out,
                 void* stream) {
-    if (!p || !d_raw || !d_out) return set_error(ASARF_ERR_INVALID, "focus: null argument");
+    if (!p || !d_raw || (!d_out && !p->skip_tail)) return set_error(ASARF_ERR_INVALID, "focus: null argument");
     if (reinterpret_cast<uintptr_t>(d_raw) & 1) return set_error(ASARF_ERR_INVALID, "raw buffer must be 2-byte aligned");
     void** ev = nullptr;
     if (p->timing_used < p->timing_slots) {
@@ -920,11 +864,13 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     mark();
     rc = backend_az_strided(p->a_inv, p->use_tma ? p->tmapB3 : nullptr, p->tiles1, p->n2, p->sh_st, stream);
     if (rc) return rc;
-    TailArgs t = p->a_tail;
-    t.out = d_out;
     mark();
-    rc = backend_tail(t, p->out_rows_max, p->sh_tail, &p->state->errors, stream);
-    if (rc) return rc;
+    if (!p->skip_tail) {
+        TailArgs t = p->a_tail;
+        t.out = d_out;
+        rc = backend_tail(t, p->out_rows_max, p->sh_tail, &p->state->errors, stream);
+        if (rc) return rc;
+    }
     mark();
     return ASARF_OK;
 }

@@ -4,6 +4,7 @@
 #include <complex>
 #include <vector>
 
+#include "asarf.h"
 #include "fft.cuh"
 
 namespace asarf {
@@ -16,6 +17,12 @@ struct HostFft {
 };
 
 bool smooth(int n);
+// Longest synthetic aperture in lines over the range swath (CalcAperturePixels).
+int max_aperture_pixels(const asarf_scene& s);
+// Ground-to-slant SRGR polynomial (5 coefficients) and ground sample count for a multilooked
+// block of azimuth_size lines at line interval lti (SlantRangeToGroundRangeInterpolation setup).
+int srgr_poly(const asarf_scene& s, double slant_first, int range_size, int azimuth_size, double lti, double poly[5],
+              int* ng);
 bool build_fft(int n, HostFft& h);
 int choose_rc_len(int nr);
 int32_t fft_size_above(int32_t v);

@@ -110,6 +110,7 @@ struct AzStridedArgs {
     int inverse;
     int use_tma;          // tile loaded by TMA (device only)
     int n1_box;           // rows per TMA box (n1 split into n1 / n1_box boxes of <= 256 rows)
+    int out_row0;         // inverse: row r is stored at out + (r - out_row0) * pitch
 };
 
 // Per range column constants of the range-Doppler block.

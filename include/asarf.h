@@ -228,6 +228,44 @@ int asarf_batch_focus(asarf_batch* batch, const uint8_t* const* d_raw, const uin
 int asarf_lpt_assign(const int64_t* work, int32_t n, int32_t bins, int32_t* out_bin);
 
 /* ---------------------------------------------------------------------------------------
+ * Long strips as overlapped azimuth blocks.  No reference counterpart: the reference focuses
+ * a scene as one padded image and does not support an azimuth-varying Doppler centroid.
+ * Blocks of block_lines lines start (block_lines - overlap) apart (the last one ends at the
+ * strip's last line); each is an ordinary plan with its own IQ statistics, Doppler estimate
+ * and Vr (from the orbit at its own azimuth time unless the scene gives Vr), and writes the lines between the
+ * midpoints of its overlaps (past one synthetic aperture at the strip ends) into one strip
+ * SLC; one multilook + RSL + SRGR pass then runs over the whole strip.  overlap must be at
+ * least the synthetic aperture in lines.
+ * ------------------------------------------------------------------------------------- */
+typedef struct asarf_strip asarf_strip;
+
+typedef struct asarf_strip_dims {
+    int32_t n_blocks, block_lines, overlap;
+    int32_t first_line;        /* strip line of the first SLC row */
+    int32_t slc_rows, slc_cols, slc_pitch;
+    int32_t out_rows, out_cols; /* detected ground-range image, row pitch out_cols */
+    int32_t max_aperture;
+    size_t device_bytes;
+} asarf_strip_dims;
+
+int asarf_strip_create(const asarf_scene* scene, int32_t block_lines, int32_t overlap, const asarf_options* opt,
+                       asarf_strip** out);
+void asarf_strip_destroy(asarf_strip* strip);
+int asarf_strip_get_dims(const asarf_strip* strip, asarf_strip_dims* dims);
+/* Block k: first strip line, kept block-relative lines [keep_lo, keep_hi), its plan (owned by
+ * the strip; asarf_plan_results gives the block's own statistics and Doppler estimate). */
+int asarf_strip_block(const asarf_strip* strip, int32_t k, int32_t* start, int32_t* keep_lo, int32_t* keep_hi,
+                      asarf_plan** plan);
+/* Raw strip bytes [azimuth_size][raw_line_bytes] -> detected image [out_rows][out_cols].
+ * Blocks run concurrently on the strip's side streams, forked from and joined into `stream`. */
+int asarf_focus_strip(asarf_strip* strip, const uint8_t* d_raw, const uint16_t* d_swst, int32_t min_swst,
+                      float* d_out, void* stream);
+/* Copy the strip SLC, complex [slc_rows][slc_cols] (row pitch slc_cols), into d_slc. */
+int asarf_strip_slc(asarf_strip* strip, void* d_slc, void* stream);
+/* Error flags of the last run over every block and the strip tail (synchronises). */
+int asarf_strip_errors(asarf_strip* strip, uint32_t* errors, void* stream);
+
+/* ---------------------------------------------------------------------------------------
  * Per-stage entry points: the reference's sar/ functions one at a time, for a caller that
  * keeps the reference's own pipeline (main.cc) and swaps stages.  Images use the layout of
  * DevicePaddedImage (cuda_util/device_padded_image.cuh:13-27): complex float

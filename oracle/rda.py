@@ -441,6 +441,87 @@ class FocusResult:
     extra: dict = field(default_factory=dict)
 
 
+def _range_doppler_image(raw: np.ndarray, scene: dict, ref_compat: bool = True):
+    """main.cc:233-287 for one block: decode .. RangeDopplerAlgorithm.  Returns the padded
+    range-Doppler-processed image, nk, the Doppler polynomial and the Vr polynomial."""
+    nr = scene["range_size"]
+    na = scene["azimuth_size"]
+    nc = scene["chirp_samples"]
+    rg_pad, az_pad = geo.reference_padding(nr, nc, na)
+    img = pad_image(decode_ers(raw, scene["samples_per_line"], scene.get("swst"), nr), rg_pad, az_pad)
+    raw_data_correction(img, nr, na, scene["total_raw_samples"], ref_compat)
+    zero_nans(img)
+    osv = [geo.Osv(*o) for o in scene["osv"]]
+    if scene.get("vr_poly") is not None:
+        vr_poly = np.asarray(scene["vr_poly"], dtype=np.float64)
+    else:
+        vr_poly = geo.estimate_processing_velocity(
+            osv, scene["first_line_time_us"], scene["line_time_interval"], scene["center_point"],
+            scene["slant_range_first"], scene["range_spacing"], scene["carrier_frequency"],
+            scene["vr_poly_init"], scene["prf"], scene["az_bw_frac"], nr, nc, na)
+    chirp = generate_chirp(scene["chirp_kr"], scene["range_sampling_rate"], nc, scene["apply_window"], rg_pad)
+    dc_poly, _, _ = doppler_centroid(img, nr, na, scene["prf"])
+    nk = range_compression(img, na, nr, chirp, nc)
+    args = RdaArgs(scene["prf"], scene["wavelength"], scene["az_bw_frac"], scene["range_spacing"],
+                   scene["slant_range_first"], dc_poly, vr_poly)
+    return range_doppler(img, nk, na, args), nk, dc_poly, vr_poly
+
+
+def _round_away(v: float) -> int:
+    """llround: nearest integer, halves away from zero."""
+    return int(math.floor(abs(v) + 0.5)) * (1 if v >= 0 else -1)
+
+
+def strip_layout(na: int, block: int, overlap: int, max_ap: int, lines_before: int = 0, lines_after: int = 0):
+    """Block starts and kept block-relative line ranges of a strip of na lines in blocks of
+    `block` lines overlapping by `overlap` (seams at the overlap midpoints, one synthetic
+    aperture dropped at each strip end).  Returns (starts, keep_lo, keep_hi, first_line)."""
+    B = min(block, na)
+    nb = 1 if na <= B else 1 + (na - B + (B - overlap) - 1) // (B - overlap)
+    starts = [min(k * (B - overlap), na - B) for k in range(nb)]
+    sm, em = max(lines_before, max_ap), max(lines_after, max_ap)
+    lo, hi = [], []
+    for k, s in enumerate(starts):
+        lo.append(sm if k == 0 else (starts[k - 1] + B + s) // 2 - s)
+        hi.append(B - em if k == nb - 1 else (s + B + starts[k + 1]) // 2 - s)
+    return starts, lo, hi, sm
+
+
+def focus_strip(raw: np.ndarray, scene: dict, block: int, overlap: int, ref_compat: bool = True):
+    """Overlapped-block strip focusing: each block focused as its own scene (own statistics,
+    Doppler estimate and orbit time), its kept lines assembled into one strip SLC, then one
+    multilook + range-spreading-loss + SRGR pass over the strip.  Returns (detected, slc)."""
+    na = scene["azimuth_size"]
+    nr, nc = scene["range_size"], scene["chirp_samples"]
+    ap = geo.calc_aperture_pixels(scene["carrier_frequency"], scene["vr_poly_init"], [], scene["prf"],
+                                  scene["az_bw_frac"], scene["slant_range_first"], scene["range_spacing"], nr, nc)
+    starts, lo, hi, first = strip_layout(na, block, overlap, max(ap), scene["lines_before"], scene["lines_after"])
+    B = min(block, na)
+    parts = []
+    for s, a, b in zip(starts, lo, hi):
+        bs = dict(scene)
+        bs["azimuth_size"] = B
+        bs["total_raw_samples"] = scene["samples_per_line"] * B
+        bs["first_line_time_us"] = scene["first_line_time_us"] + _round_away(s * scene["line_time_interval"] * 1e6)
+        if scene.get("swst") is not None:
+            bs["swst"] = np.asarray(scene["swst"])[s:s + B]
+        out, nk, _, _ = _range_doppler_image(raw[s:s + B], bs, ref_compat)
+        parts.append(out[a:b, : nk])
+    nk = parts[0].shape[1]
+    half = geo.RCMC_WINDOW // 2
+    slc = np.concatenate(parts, axis=0)[:, half: nk - half]
+    ml, ratio = azimuth_multilook(slc, scene["azimuth_spacing"])
+    sub_first = scene["slant_range_first"] + half * scene["range_spacing"]
+    ml = (ml * geo.rsl_table(slc.shape[1], sub_first, scene["range_spacing"])[None, :]).astype(np.float32)
+    osv = [geo.Osv(*o) for o in scene["osv"]]
+    t0 = scene["first_line_time_us"] + _round_away(first * scene["line_time_interval"] * 1e6)
+    lti_ml = float(np.float64(1.0 / scene["prf"]) * np.float64(ratio))
+    grsr, ng = geo.srgr_polynomial(osv, t0, lti_ml, ml.shape[0], scene["center_point"], sub_first,
+                                   scene["range_spacing"], slc.shape[1])
+    start, frac = geo.srgr_index_map(grsr, scene["range_spacing"], ng)
+    return srgr(ml, start, frac), slc
+
+
 def focus(raw: np.ndarray, scene: dict, ref_compat: bool = True, keep_intermediate: bool = False) -> FocusResult:
     """main.cc:233-327 for an ERS-style byte-I/Q scene described by ``scene`` (see
     ``asarf.scene.Scene.to_dict``)."""
