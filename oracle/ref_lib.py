@@ -11,6 +11,8 @@ from pathlib import Path
 import numpy as np
 
 REF_LIB = Path(__file__).resolve().parent / "_ref" / "libasar_ref.so"
+# the same harness over the product's header-compatible drop-in (asar-focus_b200/dropin)
+DROPIN_LIB = Path(__file__).resolve().parent / "_ref" / "libasar_dropin.so"
 
 
 class RefOutputs(C.Structure):
@@ -24,31 +26,32 @@ class RefOutputs(C.Structure):
     ]
 
 
-_lib = None
+_libs: dict = {}
 
 
-def available() -> bool:
-    return REF_LIB.exists()
+def available(path: Path = REF_LIB) -> bool:
+    return path.exists()
 
 
-def load():
-    global _lib
-    if _lib is None:
-        if not REF_LIB.exists():
-            raise FileNotFoundError(f"reference build missing: {REF_LIB} (make -C oracle/ref_build)")
-        _lib = C.CDLL(str(REF_LIB))
-        f = _lib.ref_focus
+def load(path: Path = REF_LIB):
+    if path not in _libs:
+        if not path.exists():
+            raise FileNotFoundError(f"reference build missing: {path} (make -C oracle/ref_build)")
+        lib = C.CDLL(str(path))
+        f = lib.ref_focus
         f.restype = C.c_int
         f.argtypes = [C.c_void_p, C.POINTER(C.c_double * 3), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                       C.POINTER(RefOutputs), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-    return _lib
+        _libs[path] = lib
+    return _libs[path]
 
 
 def ref_focus(scene_c, vr_poly, raw: np.ndarray, swst=None, dumps: bool = False, out_capacity: int | None = None,
-              d_raw_ptr: int = 0):
-    """Run the reference chain on host raw bytes.  Returns (detected float32 [rows, cols],
-    outputs dict, dumps dict)."""
-    lib = load()
+              d_raw_ptr: int = 0, lib_path: Path = REF_LIB):
+    """Run the reference chain (main.cc's flow) on host raw bytes, through the reference's
+    own stages (REF_LIB) or through the drop-in (DROPIN_LIB).  Returns (detected float32
+    [rows, cols], outputs dict, dumps dict)."""
+    lib = load(lib_path)
     raw = np.ascontiguousarray(raw, dtype=np.uint8)
     na, nr = scene_c.azimuth_size, scene_c.range_size
     nk = nr - scene_c.chirp_samples
