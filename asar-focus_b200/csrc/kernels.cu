@@ -3,6 +3,9 @@
 
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -162,12 +165,22 @@ int check_launch(const char* what) {
     return ASARF_OK;
 }
 
+// Raise a kernel's dynamic shared-memory limit to `bytes` (once per kernel, device and size:
+// the default limit of 48 KiB counts the kernel's static shared memory too, so any dynamic
+// size is checked, not only those above 48 KiB).
 template <class K>
 int ensure_smem(K kernel, size_t bytes, const char* what) {
-    if (bytes > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-        if (e != cudaSuccess) return set_error(ASARF_ERR_CUDA, "%s smem %zu: %s", what, bytes, cudaGetErrorString(e));
-    }
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return ASARF_OK;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (e != cudaSuccess) return set_error(ASARF_ERR_CUDA, "%s smem %zu: %s", what, bytes, cudaGetErrorString(e));
+    done[key] = bytes;
     return ASARF_OK;
 }
 

@@ -148,6 +148,15 @@ def _barrier(world: int):
         dist.barrier()
 
 
+def _describe(sc) -> str:
+    kind = "ASAR IM-like" if sc.bits == 8 else "ERS-like"
+    dc = f"Doppler {sc.dc_coeffs[0]:+.0f} Hz + range terms" if sc.dc_kind == "poly" else \
+        f"Doppler drifting +-{sc.dc_drift:.0f} Hz along azimuth"
+    grid = f"{sc.grid[0]}x{sc.grid[1]} point grid"
+    vr = "Vr from the orbit state vectors" if sc.vr_given is None else f"Vr {sc.vr_given:.0f} m/s"
+    return f"{kind} {sc.range_size} range x {sc.azimuth_size} azimuth, {sc.bits}-bit I/Q, {grid}, {dc}, {vr}"
+
+
 def make_scene(workload: str, seed: int):
     from asarf import scene as S
     return S.WORKLOADS[workload](seed=seed)
@@ -286,8 +295,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32 (complex64 data, FP64 geometry)", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: ERS-like {sc.range_size} range x {sc.azimuth_size} azimuth, "
-                               f"{sc.bits}-bit I/Q, 20x20 point grid, DC 250..350 Hz, Vr from 5 orbit vectors",
+        "config": {"workload": f"{args.workload}: {_describe(sc)}",
                    "range_samples": sc.range_size, "azimuth_lines": sc.azimuth_size, "scenes_per_step": world,
                    "l2": f"inputs larger than L2 (raw {raw_np.nbytes / 1e6:.0f} MB, complex images "
                          f"{dims['az_pad'] * dims['nk'] * 8 / 1e9:.2f} GB each)",

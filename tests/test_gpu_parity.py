@@ -30,7 +30,15 @@ def _slc(plan, res):
     return d.cpu().numpy()
 
 
-@pytest.mark.parametrize("factory", [S.tiny, S.ers_small])
+def asar_small(**kw):
+    """The ENVISAT ASAR IM-like parameter set (8-bit I/Q, 27.1 us / 16 MHz chirp, PRF 1652,
+    quadratic Doppler) on a 4096-line cut."""
+    base = dict(azimuth_size=4096, grid=(4, 4))
+    base.update(kw)
+    return S.asar_im(**base)
+
+
+@pytest.mark.parametrize("factory", [S.tiny, S.ers_small, asar_small])
 def test_matches_oracle(gpu_lib, factory):
     sc, raw, _ = scene_and_raw(gpu_lib, factory)
     plan, out, res = _focus(gpu_lib, sc, raw)
@@ -109,7 +117,7 @@ def test_host_api_equals_device_api_and_is_deterministic(gpu_lib):
     assert np.array_equal(outs[0], host)
 
 
-@pytest.mark.parametrize("factory", [S.tiny, S.ers_small])
+@pytest.mark.parametrize("factory", [S.tiny, S.ers_small, asar_small])
 def test_matches_reference_build(gpu_lib, factory):
     """Against the reference's own CUDA build (cuFFT) run on this GPU."""
     from oracle import ref_lib
