@@ -531,7 +531,6 @@ ASARF_HD ASARF_INLINE void range_compress_ct_body(const RangeCompressArgs& a, in
     const FocusState& st = *a.state;
     const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
     const uint8_t* row = raw_line ? raw_line : a.raw + static_cast<long long>(y) * a.line_bytes;
-    const float2* __restrict__ tw = a.plan.tw;
     ct_phase<NTHR>(
         [&](int t) {
 #pragma unroll
@@ -544,26 +543,15 @@ ASARF_HD ASARF_INLINE void range_compress_ct_body(const RangeCompressArgs& a, in
                     const uint16_t wv = *reinterpret_cast<const uint16_t*>(row + 2ll * i);
                     z = correct_sample(wv & 0xff, wv >> 8, st);
                 }
-                s[l] = z;
+                s[ct_pad<L>(l)] = z;
             }
         },
         tid);
-    ct_fft_forward<L>(s, tw, tid);
-    ct_phase<NTHR>(
-        [&](int t) {
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                const int l = t + k * NTHR;
-                if (L % NTHR != 0 && l >= L) break;
-                s[l] = cmul(s[l], ASARF_LDG(a.mf + l));
-            }
-        },
-        tid);
-    ct_fft_inverse<L>(s, tw, tid);
+    ct_fft_mf_ifft<L>(s, a.ctw, a.mf, tid);
     float2* orow = a.out + static_cast<long long>(y) * a.out_pitch;
     ct_phase<NTHR>(
         [&](int t) {
-            for (int l = t; l < a.nk; l += NTHR) orow[l] = s[l];
+            for (int l = t; l < a.nk; l += NTHR) orow[l] = s[ct_pad<L>(l)];
         },
         tid);
 }

@@ -2,45 +2,208 @@
 //
 // The range FFT length is a free choice (any L >= range size gives the same compressed
 // samples), so the planner picks it from the lengths below and the whole transform is
-// instantiated with constant radices, spans and per-thread item counts: every index
-// computation folds to shifts and constant multiplies.  The radix order is the runtime
-// factoriser's (host.cpp `factorize`), so the digit-reversed output order - and with it the
-// matched-filter table - is identical to the generic path's.
+// instantiated with constant radices, spans and per-thread item counts.
+//
+// Each length is three passes of composite radices (8, 12, 16, 24 or 32), each pass one
+// register-resident DFT per item: three shared-memory round trips per transform instead
+// of one per radix-2..8 stage.  The last forward pass, the matched-filter multiply and the
+// first inverse pass touch the same R contiguous positions, so one thread does all three in
+// registers (no shared-memory traffic between them).  The tile is padded with one element
+// after every Q = (last radix) elements: every pass's R inputs stay at a constant stride,
+// and lanes reading blocks of Q contiguous elements fall into different banks.
+//
+// Twiddles: a per-pass table tw_I[q][j] = exp(-2 pi i j q / M_I) (q = 1..R_I-1, j < S_I,
+// M_I = R_I S_I), adjacent j adjacent in memory so a warp's loads coalesce; the matched
+// filter is stored transposed, mf[q][b] for position b*R_last + q, for the same reason.
+// The output order of the forward transform (and so the matched filter's order) is the
+// digit reversal of this radix sequence, which the host builds from ct_radices().
 #pragma once
+
+#include <type_traits>
+#include <utility>
 
 #include "fft.cuh"
 #include "hd.cuh"
 
 namespace asarf {
 
+// ----------------------------------------------------------------------------- constants
+// cos / sin of 2 pi num / den in double, evaluated at compile time from their Taylor series
+// after reduction to [0, pi/4) by the symmetries of the circle (plain mathematics).
+constexpr double ct_pi = 3.14159265358979323846264338327950288;
+
+ASARF_HD constexpr double ct_taylor_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 24; ++k) {
+        term *= -x * x / ((2 * k - 1) * (2 * k));
+        sum += term;
+    }
+    return sum;
+}
+ASARF_HD constexpr double ct_taylor_sin(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 24; ++k) {
+        term *= -x * x / ((2 * k) * (2 * k + 1));
+        sum += term;
+    }
+    return sum;
+}
+// 8 * num / den = octant + fraction; the fraction of the octant is exact in double
+ASARF_HD constexpr double ct_cos2pi(long num, long den) {
+    num %= den;
+    if (num < 0) num += den;
+    const long e = 8 * num;
+    const long oct = e / den;
+    const double frac = static_cast<double>(e - oct * den) / static_cast<double>(den);
+    const double x = frac * ct_pi / 4;
+    const double y = (1.0 - frac) * ct_pi / 4;
+    switch (oct) {
+        case 0: return ct_taylor_cos(x);
+        case 1: return ct_taylor_sin(y);
+        case 2: return -ct_taylor_sin(x);
+        case 3: return -ct_taylor_cos(y);
+        case 4: return -ct_taylor_cos(x);
+        case 5: return -ct_taylor_sin(y);
+        case 6: return ct_taylor_sin(x);
+        default: return ct_taylor_cos(y);
+    }
+}
+// sin(2 pi n / d) = cos(2 pi (4n - d) / 4d)
+ASARF_HD constexpr double ct_sin2pi(long num, long den) { return ct_cos2pi(4 * num - den, 4 * den); }
+
+// ----------------------------------------------------------------------------- composite DFTs
+// Compile-time loop: f(std::integral_constant<int, I>) for I = 0 .. N-1, so that indices
+// are constant expressions (twiddle constants evaluated by the compiler, never at run time).
+template <class F, int... I>
+ASARF_HD ASARF_INLINE void ct_static_for_impl(F& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+ASARF_HD ASARF_INLINE void ct_static_for(F&& f) {
+    ct_static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// a * W_R^{e} (forward W = exp(-2 pi i / R), inverse conjugate) with constant factors
+template <int R, long E, bool INV>
+ASARF_HD ASARF_INLINE float2 ct_twiddle(float2 a) {
+    if constexpr (E % R == 0) {
+        return a;
+    } else {
+        constexpr float c = static_cast<float>(ct_cos2pi(E, R));
+        constexpr float sn = static_cast<float>(INV ? ct_sin2pi(E, R) : -ct_sin2pi(E, R));
+        return cmul(a, make_float2(c, sn));
+    }
+}
+
+// X[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[n1 R2 + n2] W_R1^{n1 k1}
+// (forward W = exp(-2 pi i / R); inverse conjugate), natural order in and out.
+template <int R1, int R2, bool INV>
+ASARF_HD ASARF_INLINE void dft_composite(float2* v) {
+    constexpr int R = R1 * R2;
+    float2 t[R];
+    ct_static_for<R2>([&](auto n2c) {
+        constexpr int n2 = decltype(n2c)::value;
+        float2 a[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) a[n1] = v[n1 * R2 + n2];
+        dft<R1, INV>(a);
+        ct_static_for<R1>([&](auto k1c) {
+            constexpr int k1 = decltype(k1c)::value;
+            t[k1 * R2 + n2] = ct_twiddle<R, static_cast<long>(n2) * k1, INV>(a[k1]);
+        });
+    });
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        float2 b[R2];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) b[n2] = t[k1 * R2 + n2];
+        dft<R2, INV>(b);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = b[k2];
+    }
+}
+
+template <int R, bool INV>
+ASARF_HD ASARF_INLINE void dft_ct(float2* v) {
+    if constexpr (R == 12) dft_composite<4, 3, INV>(v);
+    else if constexpr (R == 16) dft_composite<4, 4, INV>(v);
+    else if constexpr (R == 24) dft_composite<8, 3, INV>(v);
+    else if constexpr (R == 32) dft_composite<8, 4, INV>(v);
+    else dft<R, INV>(v);
+}
+
+// ----------------------------------------------------------------------------- schedules
 template <int L>
 struct CtSchedule {
     static constexpr int count = 0;
 };
-#define ASARF_CT_SCHEDULE(LEN, NT, ...)                   \
-    template <>                                           \
-    struct CtSchedule<LEN> {                              \
-        static constexpr int r[] = {__VA_ARGS__};         \
-        static constexpr int count = sizeof(r) / sizeof(int); \
-        static constexpr int nthr = NT;                   \
+#define ASARF_CT_SCHEDULE(LEN, NT, R0, R1, R2)   \
+    template <>                                  \
+    struct CtSchedule<LEN> {                     \
+        static constexpr int r[] = {R0, R1, R2}; \
+        static constexpr int count = 3;          \
+        static constexpr int nthr = NT;          \
     }
-ASARF_CT_SCHEDULE(768, 256, 8, 8, 4, 3);
-ASARF_CT_SCHEDULE(1024, 256, 8, 8, 8, 2);
-ASARF_CT_SCHEDULE(1536, 256, 8, 8, 8, 3);
-ASARF_CT_SCHEDULE(2048, 256, 8, 8, 8, 4);
-ASARF_CT_SCHEDULE(3072, 384, 8, 8, 8, 2, 3);
-ASARF_CT_SCHEDULE(4096, 512, 8, 8, 8, 8);
-ASARF_CT_SCHEDULE(6144, 512, 8, 8, 8, 4, 3);
-ASARF_CT_SCHEDULE(8192, 512, 8, 8, 8, 8, 2);
+ASARF_CT_SCHEDULE(768, 96, 8, 8, 12);
+ASARF_CT_SCHEDULE(1024, 128, 8, 8, 16);
+ASARF_CT_SCHEDULE(1536, 192, 24, 8, 8);
+ASARF_CT_SCHEDULE(2048, 128, 16, 16, 8);
+ASARF_CT_SCHEDULE(3072, 256, 16, 16, 12);
+ASARF_CT_SCHEDULE(4096, 256, 16, 16, 16);
+ASARF_CT_SCHEDULE(6144, 384, 24, 16, 16);
+ASARF_CT_SCHEDULE(8192, 256, 16, 16, 32);
 #undef ASARF_CT_SCHEDULE
 
 constexpr int kCtLengths[] = {768, 1024, 1536, 2048, 3072, 4096, 6144, 8192};
+
+// Radix sequence of a compile-time length (host: digit reversal, matched filter, tables).
+inline int ct_radices(int L, int* out) {
+    auto put = [&](const int* r) {
+        for (int i = 0; i < 3; ++i) out[i] = r[i];
+        return 3;
+    };
+    switch (L) {
+        case 768: return put(CtSchedule<768>::r);
+        case 1024: return put(CtSchedule<1024>::r);
+        case 1536: return put(CtSchedule<1536>::r);
+        case 2048: return put(CtSchedule<2048>::r);
+        case 3072: return put(CtSchedule<3072>::r);
+        case 4096: return put(CtSchedule<4096>::r);
+        case 6144: return put(CtSchedule<6144>::r);
+        case 8192: return put(CtSchedule<8192>::r);
+        default: return 0;
+    }
+}
 
 template <int L, int I>
 ASARF_HD constexpr int ct_span() {
     int m = L;
     for (int k = 0; k <= I; ++k) m /= CtSchedule<L>::r[k];
     return m;
+}
+// offset of pass I's twiddle table: sum over the earlier passes of (R - 1) * S
+template <int L, int I>
+ASARF_HD constexpr int ct_tw_offset() {
+    int off = 0, m = L;
+    for (int k = 0; k < I; ++k) {
+        m /= CtSchedule<L>::r[k];
+        off += (CtSchedule<L>::r[k] - 1) * m;
+    }
+    return off;
+}
+template <int L>
+ASARF_HD constexpr int ct_padq() {
+    return CtSchedule<L>::r[CtSchedule<L>::count - 1];
+}
+// padded shared-memory index of transform position e
+template <int L>
+ASARF_HD ASARF_INLINE int ct_pad(int e) {
+    return e + e / ct_padq<L>();
+}
+// host: padded tile elements of a compile-time length
+inline int ct_smem_elems_of(int L) {
+    int r[3];
+    return ct_radices(L, r) ? L + L / r[2] : 0;
 }
 
 // Run `phase(tid)` for this thread and barrier (device), or for every thread in turn (host
@@ -56,78 +219,85 @@ ASARF_HD ASARF_INLINE void ct_phase(F&& phase, int tid) {
 #endif
 }
 
-template <int L, int NTHR, int R, int S, bool INV, bool DIT>
-ASARF_HD ASARF_INLINE void ct_stage(float2* s, const float2* __restrict__ tw, int tid) {
+// One pass I < count-1 (span S > 1, a multiple of Q): forward DIF (DFT, then twiddle output q
+// by W_M^{jq}) or inverse DIT (conjugate twiddles on the inputs, then the inverse DFT).
+template <int L, int I, bool INV>
+ASARF_HD ASARF_INLINE void ct_pass(float2* s, const float2* __restrict__ ctw, int t) {
+    constexpr int NTHR = CtSchedule<L>::nthr;
+    constexpr int R = CtSchedule<L>::r[I];
+    constexpr int S = ct_span<L, I>();
     constexpr int M = S * R;
+    constexpr int Q = ct_padq<L>();
     constexpr int ITEMS = L / R;
-    constexpr int TW_STEP = L / M;
     constexpr int PER = (ITEMS + NTHR - 1) / NTHR;
+    constexpr int STRIDE = S + S / Q;  // padded distance between a butterfly's inputs
+    constexpr int TWO = ct_tw_offset<L, I>();
+    static_assert(S % Q == 0, "every pass but the last has a span divisible by the pad quotient");
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-        const int t = tid + k * NTHR;
-        if (ITEMS % NTHR != 0 && t >= ITEMS) break;
-        const int b = t / S;
-        const int j = t - b * S;
-        float2* p = s + b * M + j;
+        const int it = t + k * NTHR;
+        if (ITEMS % NTHR != 0 && it >= ITEMS) break;
+        const int b = it / S;
+        const int j = it - b * S;
+        float2* p = s + ct_pad<L>(b * M + j);
         float2 v[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) v[m] = p[m * S];
-        if (DIT) {  // inverse, decimation in time: twiddle inputs, then the small DFT
+        for (int m = 0; m < R; ++m) v[m] = p[m * STRIDE];
+        if (INV) {
             if (j != 0) {
-                const float2 w1 = ASARF_LDG(tw + j * TW_STEP);
-                float2 w = w1;
 #pragma unroll
-                for (int q = 1; q < R; ++q) {
-                    v[q] = cmulc(v[q], w);
-                    w = cmul(w, w1);
-                }
+                for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], ASARF_LDG(ctw + TWO + (q - 1) * S + j));
             }
-            dft<R, true>(v);
-        } else {  // forward, decimation in frequency: small DFT, then twiddle outputs
-            dft<R, INV>(v);
+            dft_ct<R, true>(v);
+        } else {
+            dft_ct<R, false>(v);
             if (j != 0) {
-                const float2 w1 = ASARF_LDG(tw + j * TW_STEP);
-                float2 w = w1;
 #pragma unroll
-                for (int q = 1; q < R; ++q) {
-                    v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
-                    w = cmul(w, w1);
-                }
+                for (int q = 1; q < R; ++q) v[q] = cmul(v[q], ASARF_LDG(ctw + TWO + (q - 1) * S + j));
             }
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) p[m * S] = v[m];
+        for (int m = 0; m < R; ++m) p[m * STRIDE] = v[m];
     }
 }
 
-template <int L, int I>
-ASARF_HD ASARF_INLINE void ct_forward_from(float2* s, const float2* __restrict__ tw, int tid) {
-    if constexpr (I < CtSchedule<L>::count) {
-        constexpr int NTHR = CtSchedule<L>::nthr;
-        ct_phase<NTHR>([&](int t) { ct_stage<L, NTHR, CtSchedule<L>::r[I], ct_span<L, I>(), false, false>(s, tw, t); },
-                       tid);
-        ct_forward_from<L, I + 1>(s, tw, tid);
-    }
-}
-
-template <int L, int I>
-ASARF_HD ASARF_INLINE void ct_inverse_from(float2* s, const float2* __restrict__ tw, int tid) {
-    if constexpr (I >= 0) {
-        constexpr int NTHR = CtSchedule<L>::nthr;
-        ct_phase<NTHR>([&](int t) { ct_stage<L, NTHR, CtSchedule<L>::r[I], ct_span<L, I>(), true, true>(s, tw, t); },
-                       tid);
-        ct_inverse_from<L, I - 1>(s, tw, tid);
-    }
-}
-
-// Forward DIF (natural -> digit-reversed) and inverse DIT (digit-reversed -> natural).
+// Last forward pass, matched filter, first inverse pass: blocks of R contiguous positions
+// (span 1, no twiddles), all in registers.  mf is transposed: position b*R + q at q*(L/R) + b.
 template <int L>
-ASARF_HD ASARF_INLINE void ct_fft_forward(float2* s, const float2* __restrict__ tw, int tid) {
-    ct_forward_from<L, 0>(s, tw, tid);
+ASARF_HD ASARF_INLINE void ct_middle(float2* s, const float2* __restrict__ mf, int t) {
+    constexpr int NTHR = CtSchedule<L>::nthr;
+    constexpr int R = ct_padq<L>();
+    constexpr int ITEMS = L / R;
+    constexpr int PER = (ITEMS + NTHR - 1) / NTHR;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int b = t + k * NTHR;
+        if (ITEMS % NTHR != 0 && b >= ITEMS) break;
+        float2* p = s + b * (R + 1);  // padded position of b * R
+        float2 v[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[m] = p[m];
+        dft_ct<R, false>(v);
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cmul(v[q], ASARF_LDG(mf + q * ITEMS + b));
+        dft_ct<R, true>(v);
+#pragma unroll
+        for (int m = 0; m < R; ++m) p[m] = v[m];
+    }
 }
+
+// Forward transform, matched filter, inverse transform of the padded tile s (natural order
+// in, natural order out, unscaled); every pass ends with a barrier.
 template <int L>
-ASARF_HD ASARF_INLINE void ct_fft_inverse(float2* s, const float2* __restrict__ tw, int tid) {
-    ct_inverse_from<L, CtSchedule<L>::count - 1>(s, tw, tid);
+ASARF_HD ASARF_INLINE void ct_fft_mf_ifft(float2* s, const float2* __restrict__ ctw, const float2* __restrict__ mf,
+                                          int tid) {
+    constexpr int NTHR = CtSchedule<L>::nthr;
+    static_assert(CtSchedule<L>::count == 3, "three-pass schedules");
+    ct_phase<NTHR>([&](int t) { ct_pass<L, 0, false>(s, ctw, t); }, tid);
+    ct_phase<NTHR>([&](int t) { ct_pass<L, 1, false>(s, ctw, t); }, tid);
+    ct_phase<NTHR>([&](int t) { ct_middle<L>(s, mf, t); }, tid);
+    ct_phase<NTHR>([&](int t) { ct_pass<L, 1, true>(s, ctw, t); }, tid);
+    ct_phase<NTHR>([&](int t) { ct_pass<L, 0, true>(s, ctw, t); }, tid);
 }
 
 }  // namespace asarf

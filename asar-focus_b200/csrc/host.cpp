@@ -12,6 +12,7 @@
 #include "asarf.h"
 #include "backend.h"
 #include "bodies.cuh"
+#include "fft_ct.cuh"
 #include "internal.h"
 #include "plan.h"
 
@@ -309,9 +310,12 @@ int32_t fft_size_above(int32_t v) {
     return -1;
 }
 
-bool build_fft(int n, HostFft& h) {
-    auto f = factorize(n);
-    if (f.empty() || static_cast<int>(f.size()) > kMaxStages) return false;
+bool build_fft(int n, HostFft& h) { return build_fft_radices(n, factorize(n), h); }
+
+bool build_fft_radices(int n, const std::vector<int>& f, HostFft& h) {
+    long long prod = 1;
+    for (int r : f) prod *= r;
+    if (f.empty() || prod != n || static_cast<int>(f.size()) > kMaxStages) return false;
     h.plan.n = n;
     h.plan.nst = static_cast<int>(f.size());
     int M = n;
@@ -498,8 +502,12 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
             return set_error(ASARF_ERR_INVALID, "azimuth FFT size %d cannot be split", N);
         }
     }
-    if (!build_fft(p->rc_len, p->rc) || !build_fft(p->n1, p->f1) || !build_fft(p->n2, p->f2) ||
-        !build_fft(p->az_pad, p->fN)) {
+    // compile-time lengths use their own three-pass radix sequence (and so its output order)
+    int ctr[3];
+    const int n_ctr = ct_radices(p->rc_len, ctr);
+    const bool rc_ok = n_ctr ? build_fft_radices(p->rc_len, std::vector<int>(ctr, ctr + n_ctr), p->rc)
+                             : build_fft(p->rc_len, p->rc);
+    if (!rc_ok || !build_fft(p->n1, p->f1) || !build_fft(p->n2, p->f2) || !build_fft(p->az_pad, p->fN)) {
         delete p;
         return set_error(ASARF_ERR_INVALID, "FFT schedule failed");
     }
@@ -535,6 +543,25 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     generate_chirp(s.chirp_kr, s.range_sampling_rate, p->nc, s.apply_window != 0, p->rc_len, chirp);
     std::vector<float2> mf;
     matched_filter_table(chirp.data(), p->nc, p->rc, mf);
+    std::vector<float2> ctw;
+    if (n_ctr) {
+        // transposed filter (position b*R + q at q*(L/R) + b) and the per-pass twiddle tables
+        const int L = p->rc_len, R = ctr[n_ctr - 1], nb = L / R;
+        std::vector<float2> t(mf.size());
+        for (int b = 0; b < nb; ++b)
+            for (int q = 0; q < R; ++q) t[static_cast<size_t>(q) * nb + b] = mf[static_cast<size_t>(b) * R + q];
+        mf.swap(t);
+        int m = L;
+        for (int k = 0; k + 1 < n_ctr; ++k) {
+            const int S = m / ctr[k], M = m;
+            for (int q = 1; q < ctr[k]; ++q)
+                for (int j = 0; j < S; ++j) {
+                    const double a = -2.0 * kPi * static_cast<double>(static_cast<long long>(j) * q % M) / M;
+                    ctw.push_back(make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a))));
+                }
+            m = S;
+        }
+    }
 
     // results-window variants (CalcResultsWindow, main_flow.cc:155-201) and their tails
     const int max_ap = max_aperture_pixels(s);
@@ -586,6 +613,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     p->out_dev = p->alloc<float>(static_cast<size_t>(p->out_rows_max) * p->out_cols_max);
     float2* rc_tw = p->alloc<float2>(p->rc_len);
     p->rc_mf = p->alloc<float2>(p->rc_len);
+    float2* ct_tw = ctw.empty() ? nullptr : p->alloc<float2>(ctw.size());
     float2* tw1 = p->alloc<float2>(p->n1);
     int* drev1 = p->alloc<int>(p->n1);
     float2* tw2 = p->alloc<float2>(p->n2);
@@ -606,6 +634,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     rc = 0;
     rc |= mem_h2d(rc_tw, p->rc.tw.data(), sizeof(float2) * p->rc_len, nullptr);
     rc |= mem_h2d(p->rc_mf, mf.data(), sizeof(float2) * p->rc_len, nullptr);
+    if (ct_tw) rc |= mem_h2d(ct_tw, ctw.data(), sizeof(float2) * ctw.size(), nullptr);
     rc |= mem_h2d(tw1, p->f1.tw.data(), sizeof(float2) * p->n1, nullptr);
     rc |= mem_h2d(drev1, p->f1.drev.data(), sizeof(int) * p->n1, nullptr);
     rc |= mem_h2d(tw2, p->f2.tw.data(), sizeof(float2) * p->n2, nullptr);
@@ -672,10 +701,12 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     r.state = p->state;
     r.plan = p->rc.plan;
     r.mf = p->rc_mf;
+    r.ctw = ct_tw;
     r.nk = p->nk;
     r.out = p->bufA;
     r.out_pitch = p->pitch;
-    p->raw_smem_offset = static_cast<int>((sizeof(float2) * static_cast<size_t>(p->rc_len) + 127) / 128 * 128);
+    const int rc_elems = n_ctr ? ct_smem_elems_of(p->rc_len) : p->rc_len;  // compile-time lengths: padded tile
+    p->raw_smem_offset = static_cast<int>((sizeof(float2) * static_cast<size_t>(rc_elems) + 127) / 128 * 128);
     p->sh_rc = {512, static_cast<size_t>(p->raw_smem_offset) + (2 * static_cast<size_t>(s.samples_per_line) + 15) / 16 * 16};
 
     AzStridedArgs& f = p->a_fwd;

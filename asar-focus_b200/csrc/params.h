@@ -87,6 +87,8 @@ struct RangeCompressArgs {
     const FocusState* state;
     FftPlan plan;
     const float2* mf;     // matched filter in the forward transform's digit-reversed order, / L
+                          // (compile-time lengths: transposed, see fft_ct.cuh)
+    const float2* ctw;    // compile-time lengths: per-pass twiddle tables (fft_ct.cuh)
     int nk;
     float2* out;
     long long out_pitch;
