@@ -426,6 +426,8 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
     st.gain = gain_f;
     st.sin_c = sin_c;
     st.cos_c = cos_c;
+    st.rgain = fdiv_rn(1.0f, gain_f);
+    st.rcos = fdiv_rn(1.0f, cos_c);
     st.dc_i_d = dc_i;
     st.dc_q_d = dc_q;
     st.iq_gain = gain;
@@ -492,8 +494,9 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
 ASARF_HD ASARF_INLINE float2 correct_sample(int iv, int qv, const FocusState& st) {
     const float i1 = fsub_rn(static_cast<float>(iv), st.dc_i);
     const float q1 = fsub_rn(static_cast<float>(qv), st.dc_q);
-    const float i2 = fdiv_rn(i1, st.gain);
-    const float q2 = fdiv_rn(fma_rn(-i2, st.sin_c, q1), st.cos_c);
+    // the reference's two IEEE divisions, correctly rounded through the reciprocals
+    const float i2 = div_by_recip_rn(i1, st.gain, st.rgain);
+    const float q2 = div_by_recip_rn(fma_rn(-i2, st.sin_c, q1), st.cos_c, st.rcos);
     return make_float2(i2, q2);
 }
 
@@ -672,16 +675,6 @@ ASARF_HD ASARF_INLINE float bin_frequency(int f, int az_pad, float step) {
     return fmul_rn(static_cast<float>(k), step);
 }
 
-// Approximate quotient (2 ulp) for the interpolation weights, whose rounding never reaches a
-// branch: one reciprocal-multiply on the device.
-ASARF_HD ASARF_INLINE float fast_div(float a, float b) {
-#if defined(__CUDA_ARCH__)
-    return __fdividef(a, b);
-#else
-    return a / b;
-#endif
-}
-
 ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& cp, int x, int f, const float2* srow,
                                             int cs, unsigned int* err_flag) {
     const float prf = a.prf;
@@ -718,14 +711,14 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
                 float si = 0.0f, sq = 0.0f, nrm = 0.0f;
 #pragma unroll
                 for (int i = 0; i < kRcmcTaps; ++i) {
-                    const float wgt = fast_div((i & 1) ? -kWin[i] : kWin[i], fsub_rn(off, static_cast<float>(i)));
+                    const float wgt = ((i & 1) ? -kWin[i] : kWin[i]) * rcp_approx(fsub_rn(off, static_cast<float>(i)));
                     const float2 d = srow[first + i];
                     si = fma_rn(d.x, wgt, si);
                     sq = fma_rn(d.y, wgt, sq);
                     nrm = fadd_rn(nrm, wgt);
                 }
                 if (nrm != 0.0f) {
-                    const float inv = fast_div(1.0f, nrm);
+                    const float inv = rcp_approx(nrm);
                     out = make_float2(fmul_rn(si, inv), fmul_rn(sq, inv));
                 }
             }

@@ -106,6 +106,17 @@ ASARF_HD ASARF_INLINE void sincos_reduced(float x, float* s, float* c) {
 #endif
 }
 
+// Hardware reciprocal approximation (about 1 ulp, flush-to-zero); the host emulation divides.
+ASARF_HD ASARF_INLINE float rcp_approx(float x) {
+#if defined(__CUDA_ARCH__)
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return 1.0f / x;
+#endif
+}
+
 ASARF_HD ASARF_INLINE float rint_f(float x) {
 #if defined(__CUDA_ARCH__)
     return rintf(x);

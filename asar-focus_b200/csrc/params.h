@@ -24,6 +24,7 @@ struct StatAccum {
 // Per-column-independent output of the statistics finalisation, read by later kernels.
 struct FocusState {
     float dc_i, dc_q, gain, sin_c, cos_c;  // IQ correction as the reference applies it
+    float rgain, rcos;                     // RN(1 / gain), RN(1 / cos_c): exact divisions by reciprocal
     float dc_poly32[3];                    // Doppler centroid polynomial (float, highest power first)
     double dc_poly[3];                     // polynomial in use (estimate or the caller's)
     double dc_est[3];                      // ACCC estimate
