@@ -118,6 +118,17 @@ class FocusPlan:
         _lib.check(self.lib, self.lib.asarf_focus_host(self._h, raw_ptr, swst_ptr or None, int(min_swst), out_ptr,
                                                        C.c_void_p(stream)), "focus_host")
 
+    def focus_host_async(self, raw_ptr: int, out_ptr: int, swst_ptr: int = 0, min_swst: int = 0, stream: int = 0):
+        """asarf_focus_host_async: enqueue upload, focus and download and return at once
+        (stream 0: the plan's own non-blocking stream).  Host buffers should be pinned and
+        stay untouched until ``wait()``."""
+        _lib.check(self.lib, self.lib.asarf_focus_host_async(self._h, raw_ptr, swst_ptr or None, int(min_swst),
+                                                             out_ptr, C.c_void_p(stream)), "focus_host_async")
+
+    def wait(self):
+        """asarf_plan_wait: block until this plan's enqueued host runs have finished."""
+        _lib.check(self.lib, self.lib.asarf_plan_wait(self._h), "plan_wait")
+
     def results(self, stream: int = 0) -> dict:
         r = _lib.Results()
         _lib.check(self.lib, self.lib.asarf_plan_results(self._h, C.byref(r), C.c_void_p(stream)), "plan_results")

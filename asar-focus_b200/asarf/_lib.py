@@ -95,6 +95,8 @@ _SIGS = {
     "asarf_plan_dims": (C.c_int, [C.c_void_p, C.POINTER(Dims)]),
     "asarf_focus": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "asarf_focus_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "asarf_focus_host_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "asarf_plan_wait": (C.c_int, [C.c_void_p]),
     "asarf_plan_slc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "asarf_plan_results": (C.c_int, [C.c_void_p, C.POINTER(Results), C.c_void_p]),
     "asarf_plan_enable_timing": (C.c_int, [C.c_void_p, C.c_int32]),

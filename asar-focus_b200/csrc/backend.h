@@ -46,6 +46,7 @@ void* event_create();
 void event_destroy(void* e);
 int event_record(void* e, void* stream);
 int event_elapsed(void* a, void* b, float* ms);
+int event_sync(void* e);
 size_t smem_optin_limit();
 // Streams, cross-stream waits and CUDA graphs (device build).  The host emulation has no
 // graphs: graphs_supported() is false there and callers run their sequence directly.

@@ -231,6 +231,7 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
 }
 
 namespace asarf {
+int event_sync(void*) { return ASARF_OK; }
 void* stream_create() { return std::calloc(1, 8); }
 void stream_destroy(void* s) { std::free(s); }
 int stream_wait_event(void*, void*) { return ASARF_OK; }

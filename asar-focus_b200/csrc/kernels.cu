@@ -378,6 +378,8 @@ int event_elapsed(void* a, void* b, float* ms) {
     return cuda_rc(e, "event elapsed");
 }
 
+int event_sync(void* e) { return cuda_rc(cudaEventSynchronize(static_cast<cudaEvent_t>(e)), "event sync"); }
+
 void* stream_create() {
     cudaStream_t s = nullptr;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {

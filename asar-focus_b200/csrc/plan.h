@@ -23,6 +23,7 @@ using asarf::TailArgs;
 using asarf::event_destroy;
 using asarf::mem_alloc;
 using asarf::mem_free;
+using asarf::stream_destroy;
 
 struct asarf_plan {
     asarf_scene scene{};
@@ -67,6 +68,10 @@ struct asarf_plan {
     bool use_tma = false;
     bool skip_tail = false;       // strip blocks: the strip runs one tail over all blocks
     int raw_smem_offset = 0;
+    // asynchronous host runs: the plan's own non-blocking stream (created on first use) and
+    // the event recorded after the last enqueued image download
+    void* own_stream = nullptr;
+    void* done = nullptr;
 
     template <class T>
     T* alloc(size_t count) {
@@ -78,6 +83,8 @@ struct asarf_plan {
         return static_cast<T*>(p);
     }
     ~asarf_plan() {
+        if (done) event_destroy(done);
+        if (own_stream) stream_destroy(own_stream);
         for (void* e : events) event_destroy(e);
         for (void* p : allocs) mem_free(p);
     }

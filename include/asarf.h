@@ -131,6 +131,20 @@ int asarf_focus(asarf_plan* plan, const uint8_t* d_raw, const uint16_t* d_swst, 
 int asarf_focus_host(asarf_plan* plan, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst, float* h_out,
                      void* stream);
 
+/* The work of asarf_focus_host (raw and SWST upload, focus run, image download), enqueued on
+ * `stream` -- or, when stream is NULL, on the plan's own non-blocking stream -- and returned
+ * from without waiting.  With page-locked host buffers the copies are asynchronous, so
+ * scenes submitted to different plans overlap: one scene's upload and another's download
+ * run on the copy engines while a third is focused.  Neither host buffer may be touched,
+ * nor asarf_plan_results read, until asarf_plan_wait(plan) has returned.  Main.cc's
+ * per-file flow (main.cc:233-327) runs one scene per process; this is its multi-scene form. */
+int asarf_focus_host_async(asarf_plan* plan, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst,
+                           float* h_out, void* stream);
+
+/* Block until everything asarf_focus_host_async last enqueued on this plan has finished
+ * (immediately when nothing was enqueued). */
+int asarf_plan_wait(asarf_plan* plan);
+
 /* Copy the complex subset SLC (IMS tail input) of the last run: complex float
  * [n_lines][slc_cols] into d_slc (row pitch slc_cols).  Asynchronous. */
 int asarf_plan_slc(asarf_plan* plan, void* d_slc, void* stream);
