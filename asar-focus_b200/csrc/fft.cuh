@@ -12,11 +12,15 @@
 // Pairing the two removes every reordering pass: a frequency-domain operation (chirp
 // matched filter, RCMC, azimuth matched filter) only needs to know which frequency each
 // position holds.  Radices 2, 3, 4, 5, 7 and 8 cover all 2^a 3^b 5^c 7^d lengths the
-// range / azimuth padding rules produce.  Twiddles come from a per-length table
+// range / azimuth padding rules produce; the register-resident range transforms add
+// composite radices built from two of them (dft_any).  Twiddles come from a per-length table
 // tw[m] = exp(-2*pi*i*m/n), m in [0, n), computed in FP64 on the host.
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <type_traits>
+#include <utility>
 
 #include "hd.cuh"
 
@@ -161,6 +165,112 @@ ASARF_HD ASARF_INLINE void dft(float2* v) {
     else if constexpr (R == 8) dft8<INV>(v);
 }
 
+// ----------------------------------------------------------------------------- constants
+// cos / sin of 2 pi num / den in double, evaluated at compile time from their Taylor series
+// after reduction to [0, pi/4) by the symmetries of the circle (plain mathematics).
+constexpr double ct_pi = 3.14159265358979323846264338327950288;
+
+ASARF_HD constexpr double ct_taylor_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 24; ++k) {
+        term *= -x * x / ((2 * k - 1) * (2 * k));
+        sum += term;
+    }
+    return sum;
+}
+ASARF_HD constexpr double ct_taylor_sin(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 24; ++k) {
+        term *= -x * x / ((2 * k) * (2 * k + 1));
+        sum += term;
+    }
+    return sum;
+}
+// 8 * num / den = octant + fraction; the fraction of the octant is exact in double
+ASARF_HD constexpr double ct_cos2pi(long num, long den) {
+    num %= den;
+    if (num < 0) num += den;
+    const long e = 8 * num;
+    const long oct = e / den;
+    const double frac = static_cast<double>(e - oct * den) / static_cast<double>(den);
+    const double x = frac * ct_pi / 4;
+    const double y = (1.0 - frac) * ct_pi / 4;
+    switch (oct) {
+        case 0: return ct_taylor_cos(x);
+        case 1: return ct_taylor_sin(y);
+        case 2: return -ct_taylor_sin(x);
+        case 3: return -ct_taylor_cos(y);
+        case 4: return -ct_taylor_cos(x);
+        case 5: return -ct_taylor_sin(y);
+        case 6: return ct_taylor_sin(x);
+        default: return ct_taylor_cos(y);
+    }
+}
+// sin(2 pi n / d) = cos(2 pi (4n - d) / 4d)
+ASARF_HD constexpr double ct_sin2pi(long num, long den) { return ct_cos2pi(4 * num - den, 4 * den); }
+
+// ----------------------------------------------------------------------------- composite DFTs
+// Compile-time loop: f(std::integral_constant<int, I>) for I = 0 .. N-1, so that indices
+// are constant expressions (twiddle constants evaluated by the compiler, never at run time).
+template <class F, int... I>
+ASARF_HD ASARF_INLINE void ct_static_for_impl(F& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+ASARF_HD ASARF_INLINE void ct_static_for(F&& f) {
+    ct_static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// a * W_R^{e} (forward W = exp(-2 pi i / R), inverse conjugate) with constant factors
+template <int R, long E, bool INV>
+ASARF_HD ASARF_INLINE float2 ct_twiddle(float2 a) {
+    if constexpr (E % R == 0) {
+        return a;
+    } else {
+        constexpr float c = static_cast<float>(ct_cos2pi(E, R));
+        constexpr float sn = static_cast<float>(INV ? ct_sin2pi(E, R) : -ct_sin2pi(E, R));
+        return cmul(a, make_float2(c, sn));
+    }
+}
+
+// X[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[n1 R2 + n2] W_R1^{n1 k1}
+// (forward W = exp(-2 pi i / R); inverse conjugate), natural order in and out.
+template <int R1, int R2, bool INV>
+ASARF_HD ASARF_INLINE void dft_composite(float2* v) {
+    constexpr int R = R1 * R2;
+    float2 t[R];
+    ct_static_for<R2>([&](auto n2c) {
+        constexpr int n2 = decltype(n2c)::value;
+        float2 a[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) a[n1] = v[n1 * R2 + n2];
+        dft<R1, INV>(a);
+        ct_static_for<R1>([&](auto k1c) {
+            constexpr int k1 = decltype(k1c)::value;
+            t[k1 * R2 + n2] = ct_twiddle<R, static_cast<long>(n2) * k1, INV>(a[k1]);
+        });
+    });
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        float2 b[R2];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) b[n2] = t[k1 * R2 + n2];
+        dft<R2, INV>(b);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = b[k2];
+    }
+}
+
+// Any radix the schedules use: the direct small DFTs, or a composite of two of them.
+template <int R, bool INV>
+ASARF_HD ASARF_INLINE void dft_any(float2* v) {
+    if constexpr (R == 12) dft_composite<4, 3, INV>(v);
+    else if constexpr (R == 16) dft_composite<4, 4, INV>(v);
+    else if constexpr (R == 24) dft_composite<8, 3, INV>(v);
+    else if constexpr (R == 32) dft_composite<8, 4, INV>(v);
+    else dft<R, INV>(v);
+}
+
 // ----------------------------------------------------------------------------- one stage
 // Butterfly item t -> (column c = t % ncol, butterfly bj = t / ncol); bj -> (block b, offset j).
 // Forward (DIF): load R values at stride S, small DFT, multiply output q by W_M^{j q}.
@@ -268,8 +378,10 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
             u[m] = make_float2(q.x, q.y);
             v[m] = make_float2(q.z, q.w);
         }
+        // W_M^{j q}: one table load, higher powers by recurrence (error ~ q ulp); a table load
+        // per q is exact but measured slower
+        const float2 w1 = j != 0 ? ASARF_LDG(tw + j * tw_step) : make_float2(1.0f, 0.0f);
         if (TW_FIRST && j != 0) {
-            const float2 w1 = ASARF_LDG(tw + j * tw_step);
             float2 w = w1;
 #pragma unroll
             for (int q = 1; q < R; ++q) {
@@ -278,10 +390,9 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
                 w = cmul(w, w1);
             }
         }
-        dft<R, INV>(u);
-        dft<R, INV>(v);
+        dft_any<R, INV>(u);
+        dft_any<R, INV>(v);
         if (!TW_FIRST && j != 0) {
-            const float2 w1 = ASARF_LDG(tw + j * tw_step);
             float2 w = w1;
 #pragma unroll
             for (int q = 1; q < R; ++q) {
@@ -295,6 +406,9 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
     }
 }
 
+// Column-pair stages take the prime-power radices only: a composite radix holds twice its
+// length in registers per column pair, which lifts the azimuth kernels from 64 to 128
+// registers per thread and halves their resident CTAs (measured slower despite fewer passes).
 template <bool INV, bool TW_FIRST>
 ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int npair,
                                                    const FastDiv& pdiv, int ldc, const float2* __restrict__ tw,

@@ -19,118 +19,10 @@
 // digit reversal of this radix sequence, which the host builds from ct_radices().
 #pragma once
 
-#include <type_traits>
-#include <utility>
-
 #include "fft.cuh"
 #include "hd.cuh"
 
 namespace asarf {
-
-// ----------------------------------------------------------------------------- constants
-// cos / sin of 2 pi num / den in double, evaluated at compile time from their Taylor series
-// after reduction to [0, pi/4) by the symmetries of the circle (plain mathematics).
-constexpr double ct_pi = 3.14159265358979323846264338327950288;
-
-ASARF_HD constexpr double ct_taylor_cos(double x) {
-    double term = 1.0, sum = 1.0;
-    for (int k = 1; k < 24; ++k) {
-        term *= -x * x / ((2 * k - 1) * (2 * k));
-        sum += term;
-    }
-    return sum;
-}
-ASARF_HD constexpr double ct_taylor_sin(double x) {
-    double term = x, sum = x;
-    for (int k = 1; k < 24; ++k) {
-        term *= -x * x / ((2 * k) * (2 * k + 1));
-        sum += term;
-    }
-    return sum;
-}
-// 8 * num / den = octant + fraction; the fraction of the octant is exact in double
-ASARF_HD constexpr double ct_cos2pi(long num, long den) {
-    num %= den;
-    if (num < 0) num += den;
-    const long e = 8 * num;
-    const long oct = e / den;
-    const double frac = static_cast<double>(e - oct * den) / static_cast<double>(den);
-    const double x = frac * ct_pi / 4;
-    const double y = (1.0 - frac) * ct_pi / 4;
-    switch (oct) {
-        case 0: return ct_taylor_cos(x);
-        case 1: return ct_taylor_sin(y);
-        case 2: return -ct_taylor_sin(x);
-        case 3: return -ct_taylor_cos(y);
-        case 4: return -ct_taylor_cos(x);
-        case 5: return -ct_taylor_sin(y);
-        case 6: return ct_taylor_sin(x);
-        default: return ct_taylor_cos(y);
-    }
-}
-// sin(2 pi n / d) = cos(2 pi (4n - d) / 4d)
-ASARF_HD constexpr double ct_sin2pi(long num, long den) { return ct_cos2pi(4 * num - den, 4 * den); }
-
-// ----------------------------------------------------------------------------- composite DFTs
-// Compile-time loop: f(std::integral_constant<int, I>) for I = 0 .. N-1, so that indices
-// are constant expressions (twiddle constants evaluated by the compiler, never at run time).
-template <class F, int... I>
-ASARF_HD ASARF_INLINE void ct_static_for_impl(F& f, std::integer_sequence<int, I...>) {
-    (f(std::integral_constant<int, I>{}), ...);
-}
-template <int N, class F>
-ASARF_HD ASARF_INLINE void ct_static_for(F&& f) {
-    ct_static_for_impl(f, std::make_integer_sequence<int, N>{});
-}
-
-// a * W_R^{e} (forward W = exp(-2 pi i / R), inverse conjugate) with constant factors
-template <int R, long E, bool INV>
-ASARF_HD ASARF_INLINE float2 ct_twiddle(float2 a) {
-    if constexpr (E % R == 0) {
-        return a;
-    } else {
-        constexpr float c = static_cast<float>(ct_cos2pi(E, R));
-        constexpr float sn = static_cast<float>(INV ? ct_sin2pi(E, R) : -ct_sin2pi(E, R));
-        return cmul(a, make_float2(c, sn));
-    }
-}
-
-// X[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[n1 R2 + n2] W_R1^{n1 k1}
-// (forward W = exp(-2 pi i / R); inverse conjugate), natural order in and out.
-template <int R1, int R2, bool INV>
-ASARF_HD ASARF_INLINE void dft_composite(float2* v) {
-    constexpr int R = R1 * R2;
-    float2 t[R];
-    ct_static_for<R2>([&](auto n2c) {
-        constexpr int n2 = decltype(n2c)::value;
-        float2 a[R1];
-#pragma unroll
-        for (int n1 = 0; n1 < R1; ++n1) a[n1] = v[n1 * R2 + n2];
-        dft<R1, INV>(a);
-        ct_static_for<R1>([&](auto k1c) {
-            constexpr int k1 = decltype(k1c)::value;
-            t[k1 * R2 + n2] = ct_twiddle<R, static_cast<long>(n2) * k1, INV>(a[k1]);
-        });
-    });
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) {
-        float2 b[R2];
-#pragma unroll
-        for (int n2 = 0; n2 < R2; ++n2) b[n2] = t[k1 * R2 + n2];
-        dft<R2, INV>(b);
-#pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = b[k2];
-    }
-}
-
-template <int R, bool INV>
-ASARF_HD ASARF_INLINE void dft_ct(float2* v) {
-    if constexpr (R == 12) dft_composite<4, 3, INV>(v);
-    else if constexpr (R == 16) dft_composite<4, 4, INV>(v);
-    else if constexpr (R == 24) dft_composite<8, 3, INV>(v);
-    else if constexpr (R == 32) dft_composite<8, 4, INV>(v);
-    else dft<R, INV>(v);
-}
 
 // ----------------------------------------------------------------------------- schedules
 template <int L>
@@ -248,9 +140,9 @@ ASARF_HD ASARF_INLINE void ct_pass(float2* s, const float2* __restrict__ ctw, in
 #pragma unroll
                 for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], ASARF_LDG(ctw + TWO + (q - 1) * S + j));
             }
-            dft_ct<R, true>(v);
+            dft_any<R, true>(v);
         } else {
-            dft_ct<R, false>(v);
+            dft_any<R, false>(v);
             if (j != 0) {
 #pragma unroll
                 for (int q = 1; q < R; ++q) v[q] = cmul(v[q], ASARF_LDG(ctw + TWO + (q - 1) * S + j));
@@ -277,10 +169,10 @@ ASARF_HD ASARF_INLINE void ct_middle(float2* s, const float2* __restrict__ mf, i
         float2 v[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) v[m] = p[m];
-        dft_ct<R, false>(v);
+        dft_any<R, false>(v);
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = cmul(v[q], ASARF_LDG(mf + q * ITEMS + b));
-        dft_ct<R, true>(v);
+        dft_any<R, true>(v);
 #pragma unroll
         for (int m = 0; m < R; ++m) p[m] = v[m];
     }

@@ -941,9 +941,11 @@ int asarf_plan_kernel_times(asarf_plan* p, float* total_ms, int32_t* runs, const
     return ASARF_OK;
 }
 
-int asarf_focus_host(asarf_plan* p, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst, float* h_out,
-                     void* stream) {
-    if (!p || !h_raw || !h_out) return set_error(ASARF_ERR_INVALID, "focus_host: null argument");
+}  // extern "C"
+
+// Raw (and SWST) upload, focus run and image download, enqueued on `stream` in that order.
+static int enqueue_host_run(asarf_plan* p, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst,
+                            float* h_out, void* stream) {
     int rc = mem_h2d(p->raw_dev, h_raw, static_cast<size_t>(p->na) * p->scene.raw_line_bytes, stream);
     if (rc) return rc;
     if (h_swst) {
@@ -952,9 +954,38 @@ int asarf_focus_host(asarf_plan* p, const uint8_t* h_raw, const uint16_t* h_swst
     }
     rc = asarf_focus(p, p->raw_dev, h_swst ? p->swst_dev : nullptr, min_swst, p->out_dev, stream);
     if (rc) return rc;
-    rc = mem_d2h(h_out, p->out_dev, sizeof(float) * static_cast<size_t>(p->out_rows_max) * p->out_cols_max, stream);
+    return mem_d2h(h_out, p->out_dev, sizeof(float) * static_cast<size_t>(p->out_rows_max) * p->out_cols_max,
+                   stream);
+}
+
+extern "C" {
+
+int asarf_focus_host(asarf_plan* p, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst, float* h_out,
+                     void* stream) {
+    if (!p || !h_raw || !h_out) return set_error(ASARF_ERR_INVALID, "focus_host: null argument");
+    const int rc = enqueue_host_run(p, h_raw, h_swst, min_swst, h_out, stream);
     if (rc) return rc;
     return stream_sync(stream);
+}
+
+int asarf_focus_host_async(asarf_plan* p, const uint8_t* h_raw, const uint16_t* h_swst, int32_t min_swst,
+                           float* h_out, void* stream) {
+    if (!p || !h_raw || !h_out) return set_error(ASARF_ERR_INVALID, "focus_host_async: null argument");
+    if (!stream) {
+        if (!p->own_stream) p->own_stream = asarf::stream_create();
+        if (!p->own_stream) return set_error(ASARF_ERR_CUDA, "focus_host_async: stream creation failed");
+        stream = p->own_stream;
+    }
+    if (!p->done) p->done = asarf::event_create();
+    if (!p->done) return set_error(ASARF_ERR_CUDA, "focus_host_async: event creation failed");
+    const int rc = enqueue_host_run(p, h_raw, h_swst, min_swst, h_out, stream);
+    if (rc) return rc;
+    return asarf::event_record(p->done, stream);
+}
+
+int asarf_plan_wait(asarf_plan* p) {
+    if (!p) return set_error(ASARF_ERR_INVALID, "plan_wait: null plan");
+    return p->done ? asarf::event_sync(p->done) : ASARF_OK;
 }
 
 int asarf_plan_results(asarf_plan* p, asarf_results* res, void* stream) {
