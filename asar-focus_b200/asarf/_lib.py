@@ -26,7 +26,12 @@ class SceneC(C.Structure):
         ("n_osv", C.c_int32), ("osv", C.POINTER(Osv)),
         ("first_line_time_us", C.c_int64), ("line_time_interval", C.c_double),
         ("center_point", C.c_double * 3), ("lines_before", C.c_int32), ("lines_after", C.c_int32),
+        ("raw_format", C.c_int32), ("fbaq_i_lut", C.POINTER(C.c_float)), ("fbaq_q_lut", C.POINTER(C.c_float)),
     ]
+
+
+RAW_ERS_BYTES = 0
+RAW_ASAR_FBAQ4 = 1
 
 
 class Options(C.Structure):
@@ -95,6 +100,9 @@ _SIGS = {
     "asarf_plan_dims": (C.c_int, [C.c_void_p, C.POINTER(Dims)]),
     "asarf_focus": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "asarf_focus_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "asarf_convert_asar_blocks": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
+    "asarf_fbaq4_index": (C.c_int32, [C.c_int32, C.c_int32]),
     "asarf_focus_host_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "asarf_plan_wait": (C.c_int, [C.c_void_p]),
     "asarf_plan_slc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

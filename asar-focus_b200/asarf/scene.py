@@ -21,7 +21,7 @@ from dataclasses import dataclass, field, replace
 
 import numpy as np
 
-from . import _lib
+from . import _lib, fbaq
 
 SOL = 299792458.0
 GM = 3.986004418e14
@@ -60,6 +60,10 @@ class Scene:
     iq_gain: float = 1.02
     iq_skew_deg: float = 2.0
     swst_codes: np.ndarray | None = None
+    # raw record format: "ers" (byte I/Q) or "fbaq4" (ENVISAT ASAR FBAQ4 blocks, synthetic tables)
+    raw_format: str = "ers"
+    fbaq_q_gain: float = 1.0               # Q table scale relative to I
+    record_samples: np.ndarray | None = None  # fbaq4: samples held by each record (default: all)
     # filled by prepare()
     osv: list = field(default_factory=list)
     center_point: tuple = (0.0, 0.0, 0.0)
@@ -85,14 +89,40 @@ class Scene:
         return SOL / self.wavelength
 
     @property
+    def swst_step(self) -> int:
+        """Range samples per SWST code step: 4 for ERS records, 1 for ASAR."""
+        return 1 if self.raw_format == "fbaq4" else 4
+
+    @property
     def samples_per_line(self) -> int:
         if self.swst_codes is None:
             return self.range_size
-        return self.range_size - 4 * int(self.swst_codes.max() - self.swst_codes.min())
+        return self.range_size - self.swst_step * int(self.swst_codes.max() - self.swst_codes.min())
 
     @property
     def raw_line_bytes(self) -> int:
+        if self.raw_format == "fbaq4":
+            return 2 + fbaq.block_bytes(self.samples_per_line)
         return 2 * self.samples_per_line
+
+    @property
+    def record_counts(self) -> np.ndarray:
+        """Samples held by each raw record."""
+        if self.record_samples is not None:
+            return np.asarray(self.record_samples, dtype=np.int64)
+        return np.full(self.azimuth_size, self.samples_per_line, dtype=np.int64)
+
+    @property
+    def total_raw_samples(self) -> int:
+        return int(self.record_counts.sum())
+
+    @property
+    def fbaq_tables(self) -> tuple[np.ndarray, np.ndarray] | None:
+        if self.raw_format != "fbaq4":
+            return None
+        if getattr(self, "_tables", None) is None:
+            self._tables = fbaq.synthetic_tables(self.fbaq_q_gain)
+        return self._tables
 
     @property
     def line_time_interval(self) -> float:
@@ -172,7 +202,7 @@ class Scene:
         s.azimuth_size = self.azimuth_size
         s.samples_per_line = self.samples_per_line
         s.raw_line_bytes = self.raw_line_bytes
-        s.total_raw_samples = self.samples_per_line * self.azimuth_size
+        s.total_raw_samples = self.total_raw_samples
         s.range_sampling_rate = self.range_sampling_rate
         s.chirp_kr = self.chirp_kr
         s.pulse_duration = self.pulse_duration
@@ -198,13 +228,18 @@ class Scene:
         s.center_point = (C.c_double * 3)(*self.center_point)
         s.lines_before = self.lines_before
         s.lines_after = self.lines_after
+        if self.raw_format == "fbaq4":
+            ti, tq = self.fbaq_tables
+            s.raw_format = _lib.RAW_ASAR_FBAQ4
+            s.fbaq_i_lut = ti.ctypes.data_as(C.POINTER(C.c_float))
+            s.fbaq_q_lut = tq.ctypes.data_as(C.POINTER(C.c_float))
         return s, arr
 
     def to_dict(self) -> dict:
         """Scene as the oracle reads it."""
         return dict(
             range_size=self.range_size, azimuth_size=self.azimuth_size, samples_per_line=self.samples_per_line,
-            total_raw_samples=self.samples_per_line * self.azimuth_size, chirp_samples=self.chirp_samples,
+            total_raw_samples=self.total_raw_samples, chirp_samples=self.chirp_samples,
             chirp_kr=self.chirp_kr, range_sampling_rate=self.range_sampling_rate, apply_window=self.apply_window,
             prf=self.prf, wavelength=self.wavelength, carrier_frequency=self.carrier_frequency,
             range_spacing=self.range_spacing, slant_range_first=self.slant_range_first,
@@ -214,6 +249,8 @@ class Scene:
             line_time_interval=self.line_time_interval, center_point=tuple(self.center_point),
             lines_before=self.lines_before, lines_after=self.lines_after,
             swst=None if self.swst_codes is None else np.asarray(self.swst_codes),
+            raw_format=self.raw_format, raw_line_bytes=self.raw_line_bytes,
+            fbaq_tables=self.fbaq_tables,
         )
 
 
@@ -283,6 +320,20 @@ def tiny(**kw) -> Scene:
     return Scene(**base)
 
 
+def asar_fbaq(**kw) -> Scene:
+    """5616 x 30000 ENVISAT ASAR IM-like scene in FBAQ4 records (synthetic instrument tables)."""
+    base = dict(name="asar_fbaq", raw_format="fbaq4", seed=1005)
+    base.update(kw)
+    return asar_im(**base)
+
+
+def tiny_fbaq(**kw) -> Scene:
+    """The small test scene in FBAQ4 records."""
+    base = dict(name="tiny_fbaq", raw_format="fbaq4", seed=8)
+    base.update(kw)
+    return tiny(**base)
+
+
 def ers_mid(**kw) -> Scene:
     """5616 x 8192 cut of the ERS scene: profiling case (complex images 324 MB, above L2)."""
     base = dict(name="ers_mid", azimuth_size=8192, grid=(10, 6))
@@ -291,7 +342,7 @@ def ers_mid(**kw) -> Scene:
 
 
 WORKLOADS = {"ers_small": ers_small, "ers_full": ers_full, "asar_im": asar_im, "asar_strip": asar_strip,
-             "tiny": tiny, "ers_mid": ers_mid}
+             "tiny": tiny, "ers_mid": ers_mid, "asar_fbaq": asar_fbaq, "tiny_fbaq": tiny_fbaq}
 
 
 def with_sizes(sc: Scene, **kw) -> Scene:

@@ -3,7 +3,8 @@
 A scene is circular complex Gaussian clutter plus a grid of point targets plus thermal
 noise, then the I/Q front-end impairments (DC bias, gain imbalance, quadrature skew) and
 quantisation to 5- or 8-bit offset-binary bytes, interleaved I,Q per sample as the ERS
-byte decoder expects.
+byte decoder expects, or adaptive 4-bit block quantisation into ENVISAT ASAR FBAQ4 records
+(``asarf.fbaq``).
 
 * point targets: exact hyperbolic range history R(eta) = sqrt(R0^2 + Vr^2 (eta-eta0)^2)
   (so range migration is present), transmitted chirp exp(j pi Kr t^2), carrier phase
@@ -21,6 +22,7 @@ import math
 import numpy as np
 import torch
 
+from . import fbaq
 from .scene import SOL, Scene
 
 
@@ -137,7 +139,8 @@ def simulate(sc: Scene, device: str | torch.device = "cpu", noise_rel: float = 0
     # ---------------------------------------------------------------- front end
     bits = sc.bits
     full = float(2 ** bits)
-    sigma_raw = 4.0 if bits == 5 else 30.0
+    fbaq4 = sc.raw_format == "fbaq4"
+    sigma_raw = 8.0 if fbaq4 else (4.0 if bits == 5 else 30.0)
     scale = sigma_raw / max(clut_std, 1e-30)
     z = field * scale
     z = z + torch.complex(torch.randn(na, nr, generator=gen, device=dev, dtype=rdt),
@@ -145,6 +148,24 @@ def simulate(sc: Scene, device: str | torch.device = "cpu", noise_rel: float = 0
     skew = math.radians(sc.iq_skew_deg)
     iv = z.real * sc.iq_gain
     qv = z.imag * math.cos(skew) + z.real * math.sin(skew)
+    truth = dict(targets=target_grid(sc), clutter_scale=scale, amp=amp)
+    if return_field:
+        truth["field"] = field
+    if fbaq4:
+        # adaptive 4-bit block quantisation of the (biased, imbalanced) I/Q; record y holds the
+        # samples from its SWST offset on
+        ivn = (iv + sc.iq_bias[0]).cpu().numpy()
+        qvn = (qv + sc.iq_bias[1]).cpu().numpy()
+        spl = sc.samples_per_line
+        if sc.swst_codes is not None:
+            sw = np.asarray(sc.swst_codes, dtype=np.int64)
+            offs = sc.swst_step * (sw - sw.min())
+            ivn = np.stack([ivn[y, offs[y]:offs[y] + spl] for y in range(na)])
+            qvn = np.stack([qvn[y, offs[y]:offs[y] + spl] for y in range(na)])
+        else:
+            ivn, qvn = ivn[:, :spl], qvn[:, :spl]
+        raw = fbaq.encode(ivn, qvn, sc.record_counts, sc.raw_line_bytes, sc.fbaq_q_gain)
+        return raw, truth
     bias = full / 2 - 0.5
     iq = torch.stack([iv + bias + sc.iq_bias[0], qv + bias + sc.iq_bias[1]], dim=-1)
     iq = torch.clamp(torch.round(iq), 0, full - 1).to(torch.uint8)
@@ -157,7 +178,4 @@ def simulate(sc: Scene, device: str | torch.device = "cpu", noise_rel: float = 0
             out[y] = iq[y, offs[y]:offs[y] + spl]
         iq = out
     raw = iq.reshape(na, -1).contiguous().cpu().numpy()
-    truth = dict(targets=targets, clutter_scale=scale, amp=amp)
-    if return_field:
-        truth["field"] = field
     return raw, truth

@@ -78,6 +78,19 @@ def convert_ers_samples(raw, samples_per_line: int, img, range_size: int, swst=N
     _lib.check(lib, rc, "convert_ers_samples")
 
 
+def convert_asar_blocks(raw, img, range_size: int, lut_i, lut_q, swst=None, min_swst: int = 0, lib=None) -> None:
+    """ConvertAsarImBlocksToComplexKernel (envisat_format/src/envisat_format_kernels.cu:160-209):
+    FBAQ4 records ``raw`` uint8 [records][record_bytes] -> rows [0, range_size) of complex
+    ``img`` (NaN where a record holds no sample); ``lut_i`` / ``lut_q``: the 4096-entry tables
+    (instrument-file order) in the same memory as ``img``."""
+    lib = lib or load_library()
+    _check_contig(raw, "raw")
+    records, record_bytes = int(raw.shape[0]), int(raw.shape[1])
+    rc = lib.asarf_convert_asar_blocks(_ptr(raw), record_bytes, records, _ptr(swst), int(min_swst), _ptr(lut_i),
+                                       _ptr(lut_q), _ptr(img), int(img.shape[1]), int(range_size), _stream(img))
+    _lib.check(lib, rc, "convert_asar_blocks")
+
+
 def raw_data_correction(img: DevicePaddedImage, n_total_samples: int, lib=None) -> dict:
     """RawDataCorrection (sar/iq_correction.cu:188-274) in place; returns the SARResults
     fields it sets."""

@@ -17,6 +17,9 @@ struct LaunchShape {
 // grid (ceil(nr / kStatsCols), ceil(na / lines_per_cta)), kStatsCols threads
 int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, void* stream);
 int backend_finalize(const FinalizeArgs& a, void* stream);
+// ASAR FBAQ4 records: FP64 statistics tiles (gx = tiles_x, gy line tiles) and their fold
+int backend_raw_stats_fbaq(const RawStatsArgs& a, int gx, int gy, void* stream);
+int backend_stats_fold(const RawStatsArgs& a, int tiles_y, void* stream);
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void* stream);
 int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream);
 int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, unsigned int* err,
@@ -25,6 +28,7 @@ int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err,
 
 // per-stage kernels
 int backend_decode(const DecodeArgs& a, long long n, void* stream);
+int backend_decode_fbaq(const DecodeFbaqArgs& a, long long n, void* stream);
 int backend_img_moments(const ImgMomentsArgs& a, int blocks, void* stream);
 int backend_iq_apply(const IqApplyArgs& a, long long n, void* stream);
 int backend_zero_nans(float2* img, long long n, void* stream);

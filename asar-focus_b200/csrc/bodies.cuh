@@ -385,6 +385,187 @@ ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by,
     }
 }
 
+// ----------------------------------------------------------------------------- FBAQ4 records
+// ENVISAT ASAR raw records (ConvertAsarImBlocksToComplexKernel,
+// envisat_format/src/envisat_format_kernels.cu:160-209): a 2-byte little-endian length L of
+// the block data, then 64-byte blocks of one block-id byte and 63 codeword bytes (I code in
+// the high nibble, Q code in the low one).  Sample r of a record is codeword byte
+// j = r + r / 63 + 1 of the block data and exists when j < L (and j lies inside the record).
+
+// Instrument-file table index of a 4-bit code of block `block`: sign-magnitude codes 0..7 are
+// levels 8..15, codes 8..15 levels 7..0 (Fbaq4IndexCalc, envisat_format/include/envisat_parse_util.cuh:75-84).
+ASARF_HD ASARF_INLINE int fbaq4_index(int block, int code) { return 256 * (code > 7 ? 15 - code : 8 + code) + block; }
+
+// Usable block-data bytes of a record: its length field, bounded by the record stride.
+ASARF_HD ASARF_INLINE int fbaq_len(const uint8_t* rec, long long line_bytes) {
+    const int len = rec[0] | (rec[1] << 8);
+    const long long room = line_bytes - 2;
+    return len < room ? len : static_cast<int>(room);
+}
+
+// Sample r >= 0 of a record through the permuted tables lut[16 * block id + code].
+ASARF_HD ASARF_INLINE bool fbaq_sample(const uint8_t* rec, int len, int r, const FastDiv& d63,
+                                       const float* __restrict__ lut_i, const float* __restrict__ lut_q, float* iv,
+                                       float* qv) {
+    const int b = static_cast<int>(fdiv_u(static_cast<unsigned int>(r), d63));
+    const int j = r + b + 1;
+    if (j >= len) return false;
+    const int id = rec[2 + 64 * b];
+    const int cw = rec[2 + j];
+    *iv = ASARF_LDG(lut_i + 16 * id + (cw >> 4));
+    *qv = ASARF_LDG(lut_q + 16 * id + (cw & 15));
+    return true;
+}
+
+// Statistics of FBAQ4 records: the sums of k_raw_stats over the decoded float samples, in
+// FP64.  Tile (bx, by) = 32 columns x kFbaqStatsLines lines; warp w of the block takes lines
+// [y0 + w * sub, y0 + (w + 1) * sub) of the tile, lane = column.  Per-lane sums are combined
+// over the warps, then over the lanes (moments: fixed pairwise tree; lag sums: per Doppler
+// block in lane order), and the tile's partials are written, not accumulated: the fold sums
+// them in a fixed order, so the statistics do not depend on scheduling.
+constexpr int kFbaqSums = 15;  // 6 moments + 9 lag sums
+struct FbaqStatsSmem {
+    int off[kFbaqStatsLines + 1];  // SWST shift of the tile's lines (and the line before)
+    int len[kFbaqStatsLines + 1];  // usable block-data bytes of those records
+    double red[kFbaqStatsWarps][kFbaqSums][32];
+};
+
+ASARF_HD ASARF_INLINE void raw_stats_fbaq_body(const RawStatsArgs& a, int bx, int by, int tid, int nthr,
+                                               FbaqStatsSmem* sm) {
+    const int y0 = by * kFbaqStatsLines;
+    const int y1 = (y0 + kFbaqStatsLines < a.na) ? y0 + kFbaqStatsLines : a.na;
+    const int ys = y0 > 0 ? y0 - 1 : 0;
+    for (int y = ys + tid; y < y1; y += nthr) {
+        sm->off[y - ys] = a.swst ? static_cast<int>(a.swst[y]) - a.min_swst : 0;
+        sm->len[y - ys] = fbaq_len(a.raw + static_cast<long long>(y) * a.line_bytes, a.line_bytes);
+    }
+    ASARF_SYNC();
+    const FastDiv d63 = make_fastdiv(63u);
+    constexpr int sub = kFbaqStatsLines / kFbaqStatsWarps;
+    for (int t = tid; t < 32 * kFbaqStatsWarps; t += nthr) {
+        const int lane = t & 31, w = t >> 5;
+        const int x = bx * 32 + lane;
+        const int wy0 = y0 + w * sub;
+        const int wy1 = (wy0 + sub < y1) ? wy0 + sub : y1;
+        double v[kFbaqSums];
+#pragma unroll
+        for (int k = 0; k < kFbaqSums; ++k) v[k] = 0.0;
+        float pi = 0.0f, pq = 0.0f;
+        bool pf = false;
+        const int start = wy0 > 0 ? wy0 - 1 : 0;
+        if (x < a.nr && wy0 < wy1) {
+            for (int yb = start; yb < wy1; yb += kStatsBatch) {
+                float iv[kStatsBatch], qv[kStatsBatch];
+                bool f[kStatsBatch];
+#pragma unroll
+                for (int u = 0; u < kStatsBatch; ++u) {
+                    const int y = yb + u;
+                    f[u] = false;
+                    iv[u] = 0.0f;
+                    qv[u] = 0.0f;
+                    if (y < wy1) {
+                        const int r = x - sm->off[y - ys];
+                        if (r >= 0)
+                            f[u] = fbaq_sample(a.raw + static_cast<long long>(y) * a.line_bytes, sm->len[y - ys], r,
+                                               d63, a.lut_i, a.lut_q, &iv[u], &qv[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kStatsBatch; ++u) {
+                    const int y = yb + u;
+                    if (y >= wy1) break;
+                    const double ci = iv[u], cq = qv[u];
+                    if (y >= wy0 && f[u]) {
+                        v[0] += 1.0;
+                        v[1] += ci;
+                        v[2] += cq;
+                        v[3] += ci * ci;
+                        v[4] += cq * cq;
+                        v[5] += ci * cq;
+                        if (y > 0 && pf) {
+                            const double ai = pi, aq = pq;
+                            v[6] += 1.0;
+                            v[7] += ai;
+                            v[8] += aq;
+                            v[9] += ci;
+                            v[10] += cq;
+                            v[11] += ai * ci;
+                            v[12] += aq * cq;
+                            v[13] += ai * cq;
+                            v[14] += aq * ci;
+                        }
+                    }
+                    pi = iv[u];
+                    pq = qv[u];
+                    pf = f[u];
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kFbaqSums; ++k) sm->red[w][k][lane] = v[k];
+    }
+    ASARF_SYNC();
+    // over the warps, in warp order (into warp 0's row)
+    for (int t = tid; t < kFbaqSums * 32; t += nthr) {
+        const int k = t >> 5, lane = t & 31;
+        double acc = sm->red[0][k][lane];
+        for (int w = 1; w < kFbaqStatsWarps; ++w) acc += sm->red[w][k][lane];
+        sm->red[0][k][lane] = acc;
+    }
+    ASARF_SYNC();
+    double* out = a.part + (static_cast<long long>(by) * a.tiles_x + bx) * a.part_slots;
+    const int b0 = static_cast<int>((bx * 32) / a.dc_step);
+    // lag sums: per Doppler block, lanes in order (before the moment tree reuses the row)
+    for (int t = tid; t < 9 * a.span; t += nthr) {
+        const int bl = t / 9, q = t - bl * 9;
+        double acc = 0.0;
+        for (int lane = 0; lane < 32; ++lane) {
+            const int x = bx * 32 + lane;
+            if (x < a.nr && x / a.dc_step == b0 + bl) acc += sm->red[0][6 + q][lane];
+        }
+        out[6 + t] = acc;
+    }
+    ASARF_SYNC();
+    // moments: pairwise tree over the 32 lanes
+    for (int h = 16; h > 0; h >>= 1) {
+        for (int t = tid; t < 6 * h; t += nthr) {
+            const int k = t / h, lane = t - k * h;
+            sm->red[0][k][lane] += sm->red[0][k][lane + h];
+        }
+        ASARF_SYNC();
+    }
+    for (int k = tid; k < 6; k += nthr) out[k] = sm->red[0][k][0];
+}
+
+// Fold of the FBAQ4 partials into FloatStatAccum: over the line tiles of every
+// column tile, then over the column tiles touching each sum, both in index order.
+ASARF_HD ASARF_INLINE void stats_fold_body(const RawStatsArgs& a, int tiles_y, int tid, int nthr) {
+    const int slots = a.part_slots;
+    for (int t = tid; t < a.tiles_x * slots; t += nthr) {
+        double acc = a.part[t];
+        for (int by = 1; by < tiles_y; ++by) acc += a.part[static_cast<long long>(by) * a.tiles_x * slots + t];
+        a.part[t] = acc;
+    }
+    ASARF_SYNC();
+    for (int t = tid; t < 6 + 9 * a.nblk; t += nthr) {
+        double acc = 0.0;
+        if (t < 6) {
+            for (int bx = 0; bx < a.tiles_x; ++bx) acc += a.part[bx * slots + t];
+            a.facc->mom[t] = acc;
+        } else {
+            const int b = (t - 6) / 9, q = (t - 6) - 9 * b;
+            const int lo = (b * a.dc_step) / 32;
+            int hi = ((b + 1) * a.dc_step - 1) / 32;
+            if (hi > a.tiles_x - 1) hi = a.tiles_x - 1;
+            for (int bx = lo; bx <= hi; ++bx) {
+                const int bl = b - (bx * 32) / a.dc_step;
+                if (bl >= 0 && bl < a.span) acc += a.part[bx * slots + 6 + 9 * bl + q];
+            }
+            a.facc->lag[b][q] = acc;
+        }
+    }
+}
+
 // ----------------------------------------------------------------------------- finalisation
 // Single-threaded: IQ statistics and correction constants exactly as RawDataCorrection
 // derives them (sar/iq_correction.cu:200-273, CalcMean/CalcStdDev of
@@ -394,12 +575,15 @@ ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by,
 ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
     const StatAccum& s = *a.acc;
     FocusState& st = *a.state;
-    const double n = static_cast<double>(s.mom[0]);
-    const double SI = static_cast<double>(s.mom[1]), SQ = static_cast<double>(s.mom[2]);
-    const double SII = static_cast<double>(s.mom[3]), SQQ = static_cast<double>(s.mom[4]);
-    const double SIQ = static_cast<double>(s.mom[5]);
+    const FloatStatAccum* fs = a.facc;
+    auto mom = [&](int k) { return fs ? fs->mom[k] : static_cast<double>(s.mom[k]); };
+    auto lag = [&](int b, int q) { return fs ? fs->lag[b][q] : static_cast<double>(s.lag[b][q]); };
+    const double n = mom(0);
+    const double SI = mom(1), SQ = mom(2);
+    const double SII = mom(3), SQQ = mom(4);
+    const double SIQ = mom(5);
     unsigned int err = 0;
-    if (s.mom[0] == 0) err |= kErrStatsEmpty;
+    if (n == 0.0) err |= kErrStatsEmpty;
     const float total = static_cast<float>(a.n_total);
     // mean: float(sum) / float(total)
     const float dc_i = static_cast<float>(SI) / total;
@@ -444,12 +628,11 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
     const int nblk = a.nblk < kMaxDcBlocks ? a.nblk : kMaxDcBlocks;
     if (a.nblk > kMaxDcBlocks) err |= kErrDcBlocks;
     for (int b = 0; b < nblk; ++b) {
-        const unsigned long long* L = s.lag[b];
-        const double np = static_cast<double>(L[0]);
-        const double sA = static_cast<double>(L[1]), sB = static_cast<double>(L[2]);
-        const double sC = static_cast<double>(L[3]), sD = static_cast<double>(L[4]);
-        const double sAC = static_cast<double>(L[5]), sBD = static_cast<double>(L[6]);
-        const double sAD = static_cast<double>(L[7]), sBC = static_cast<double>(L[8]);
+        const double np = lag(b, 0);
+        const double sA = lag(b, 1), sB = lag(b, 2);
+        const double sC = lag(b, 3), sD = lag(b, 4);
+        const double sAC = lag(b, 5), sBD = lag(b, 6);
+        const double sAD = lag(b, 7), sBC = lag(b, 8);
         double re = p * p * sAC + p * p0 * (sA + sC) + p0 * p0 * np + u * u * sBD + u * v * (sBC + sAD) +
                     u * w * (sB + sD) + v * v * sAC + v * w * (sA + sC) + w * w * np;
         const double im = p * u * (sAD - sBC) + p * w * (sA - sC) + p0 * u * (sD - sB) + p0 * v * (sC - sA);
@@ -491,30 +674,60 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
 // x < XSize - chirp_samples.  Samples the decoder leaves empty are 0 (ZeroNaNs after the
 // correction, main.cc:245).  The FFT length is any L >= XSize: outputs x < Nk only correlate
 // data samples [x, x + Nc) so they do not depend on L.
-ASARF_HD ASARF_INLINE float2 correct_sample(int iv, int qv, const FocusState& st) {
-    const float i1 = fsub_rn(static_cast<float>(iv), st.dc_i);
-    const float q1 = fsub_rn(static_cast<float>(qv), st.dc_q);
+ASARF_HD ASARF_INLINE float2 correct_sample_f(float iv, float qv, const FocusState& st) {
+    const float i1 = fsub_rn(iv, st.dc_i);
+    const float q1 = fsub_rn(qv, st.dc_q);
     // the reference's two IEEE divisions, correctly rounded through the reciprocals
     const float i2 = div_by_recip_rn(i1, st.gain, st.rgain);
     const float q2 = div_by_recip_rn(fma_rn(-i2, st.sin_c, q1), st.cos_c, st.rcos);
     return make_float2(i2, q2);
 }
 
+ASARF_HD ASARF_INLINE float2 correct_sample(int iv, int qv, const FocusState& st) {
+    return correct_sample_f(static_cast<float>(iv), static_cast<float>(qv), st);
+}
+
+// Corrected sample at range position l of line y (FMT: RawFormat; row: the line's record).
+template <int FMT>
+struct LineDecoder {
+    int off, len;
+    FastDiv d63;
+    const uint8_t* row;
+    ASARF_HD ASARF_INLINE LineDecoder(const RangeCompressArgs& a, int y, const uint8_t* raw_line) {
+        row = raw_line ? raw_line : a.raw + static_cast<long long>(y) * a.line_bytes;
+        if constexpr (FMT == kRawAsarFbaq4) {
+            off = a.swst ? static_cast<int>(a.swst[y]) - a.min_swst : 0;
+            len = fbaq_len(row, a.line_bytes);
+            d63 = make_fastdiv(63u);
+        } else {
+            off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
+            len = 0;
+        }
+    }
+    ASARF_HD ASARF_INLINE float2 operator()(const RangeCompressArgs& a, const FocusState& st, int l) const {
+        float2 z = make_float2(0.0f, 0.0f);
+        const int i = l - off;
+        if constexpr (FMT == kRawAsarFbaq4) {
+            float iv, qv;
+            if (l < a.nr && i >= 0 && fbaq_sample(row, len, i, d63, a.lut_i, a.lut_q, &iv, &qv))
+                z = correct_sample_f(iv, qv, st);
+        } else {
+            if (l < a.nr && i >= 0 && i < a.spl) {
+                const uint16_t wv = *reinterpret_cast<const uint16_t*>(row + 2ll * i);
+                z = correct_sample(wv & 0xff, wv >> 8, st);
+            }
+        }
+        return z;
+    }
+};
+
+template <int FMT = kRawErsBytes>
 ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y, int tid, int nthr, float2* s,
                                                const uint8_t* raw_line) {
     const FocusState& st = *a.state;
     const int L = a.plan.n;
-    const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
-    const uint8_t* row = raw_line ? raw_line : a.raw + static_cast<long long>(y) * a.line_bytes;
-    for (int l = tid; l < L; l += nthr) {
-        float2 z = make_float2(0.0f, 0.0f);
-        const int i = l - off;
-        if (l < a.nr && i >= 0 && i < a.spl) {
-            const uint16_t wv = *reinterpret_cast<const uint16_t*>(row + 2ll * i);
-            z = correct_sample(wv & 0xff, wv >> 8, st);
-        }
-        s[l] = z;
-    }
+    const LineDecoder<FMT> dec(a, y, raw_line);
+    for (int l = tid; l < L; l += nthr) s[l] = dec(a, st, l);
     ASARF_SYNC();
     fft_forward(a.plan, s, 1, 1, tid, nthr);
     for (int l = tid; l < L; l += nthr) s[l] = cmul(s[l], ASARF_LDG(a.mf + l));
@@ -526,27 +739,20 @@ ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y
 
 // Same transform with a compile-time schedule (lengths in kCtLengths): all loops unrolled,
 // all index arithmetic constant.
-template <int L>
+template <int L, int FMT = kRawErsBytes>
 ASARF_HD ASARF_INLINE void range_compress_ct_body(const RangeCompressArgs& a, int y, int tid, float2* s,
                                                   const uint8_t* raw_line) {
     constexpr int NTHR = CtSchedule<L>::nthr;
     constexpr int PER = (L + NTHR - 1) / NTHR;
     const FocusState& st = *a.state;
-    const int off = a.swst ? 4 * (static_cast<int>(a.swst[y]) - a.min_swst) : 0;
-    const uint8_t* row = raw_line ? raw_line : a.raw + static_cast<long long>(y) * a.line_bytes;
+    const LineDecoder<FMT> dec(a, y, raw_line);
     ct_phase<NTHR>(
         [&](int t) {
 #pragma unroll
             for (int k = 0; k < PER; ++k) {
                 const int l = t + k * NTHR;
                 if (L % NTHR != 0 && l >= L) break;
-                float2 z = make_float2(0.0f, 0.0f);
-                const int i = l - off;
-                if (l < a.nr && i >= 0 && i < a.spl) {
-                    const uint16_t wv = *reinterpret_cast<const uint16_t*>(row + 2ll * i);
-                    z = correct_sample(wv & 0xff, wv >> 8, st);
-                }
-                s[ct_pad<L>(l)] = z;
+                s[ct_pad<L>(l)] = dec(a, st, l);
             }
         },
         tid);
@@ -878,6 +1084,28 @@ ASARF_HD ASARF_INLINE void decode_item(const DecodeArgs& a, long long idx) {
     if (i >= 0 && i < a.spl) {
         const uint8_t* p = a.raw + static_cast<long long>(y) * a.line_bytes + 2ll * i;
         v = make_float2(static_cast<float>(p[0]), static_cast<float>(p[1]));
+    }
+    a.img[static_cast<long long>(y) * a.stride + x] = v;
+}
+
+// ConvertAsarImBlocksToComplexKernel (envisat_format/src/envisat_format_kernels.cu:160-209) as
+// a gather over output pixels: sample r = x - (swst[y] - min_swst) of record y through the
+// instrument-file tables, NaN where the record holds no sample.
+ASARF_HD ASARF_INLINE void decode_fbaq_item(const DecodeFbaqArgs& a, long long idx) {
+    const int y = static_cast<int>(idx / a.nr);
+    const int x = static_cast<int>(idx - static_cast<long long>(y) * a.nr);
+    const int r = x - (a.swst ? static_cast<int>(a.swst[y]) - a.min_swst : 0);
+    float2 v = make_float2(qnan_f(), qnan_f());
+    if (r >= 0) {
+        const uint8_t* rec = a.raw + static_cast<long long>(y) * a.line_bytes;
+        const int len = fbaq_len(rec, a.line_bytes);
+        const int b = r / 63;
+        const int j = r + b + 1;
+        if (j < len) {
+            const int id = rec[2 + 64 * b];
+            const int cw = rec[2 + j];
+            v = make_float2(ASARF_LDG(a.lut_i + fbaq4_index(id, cw >> 4)), ASARF_LDG(a.lut_q + fbaq4_index(id, cw & 15)));
+        }
     }
     a.img[static_cast<long long>(y) * a.stride + x] = v;
 }

@@ -29,30 +29,50 @@ int backend_raw_stats(const RawStatsArgs& a, int gx, int gy, void*) {
     return ASARF_OK;
 }
 
+int backend_raw_stats_fbaq(const RawStatsArgs& a, int gx, int gy, void*) {
+    std::vector<FbaqStatsSmem> sm(1);
+    for (int by = 0; by < gy; ++by)
+        for (int bx = 0; bx < gx; ++bx) raw_stats_fbaq_body(a, bx, by, 0, 1, sm.data());
+    return ASARF_OK;
+}
+
+int backend_stats_fold(const RawStatsArgs& a, int tiles_y, void*) {
+    stats_fold_body(a, tiles_y, 0, 1);
+    return ASARF_OK;
+}
+
 int backend_finalize(const FinalizeArgs& a, void*) {
     finalize_body(a);
     return ASARF_OK;
 }
 
-template <int L>
+template <int L, int FMT>
 static void emu_rc_ct(const RangeCompressArgs& a, int lines, float2* s) {
-    for (int y = 0; y < lines; ++y) range_compress_ct_body<L>(a, y, 0, s, nullptr);
+    for (int y = 0; y < lines; ++y) range_compress_ct_body<L, FMT>(a, y, 0, s, nullptr);
+}
+
+template <int FMT>
+static void emu_rc(const RangeCompressArgs& a, int lines, LaunchShape sh) {
+    std::vector<float2> s(sh.smem / sizeof(float2) + 1);
+    switch (a.plan.n) {
+        case 768: emu_rc_ct<768, FMT>(a, lines, s.data()); return;
+        case 1024: emu_rc_ct<1024, FMT>(a, lines, s.data()); return;
+        case 1536: emu_rc_ct<1536, FMT>(a, lines, s.data()); return;
+        case 2048: emu_rc_ct<2048, FMT>(a, lines, s.data()); return;
+        case 3072: emu_rc_ct<3072, FMT>(a, lines, s.data()); return;
+        case 4096: emu_rc_ct<4096, FMT>(a, lines, s.data()); return;
+        case 6144: emu_rc_ct<6144, FMT>(a, lines, s.data()); return;
+        case 8192: emu_rc_ct<8192, FMT>(a, lines, s.data()); return;
+        default: break;
+    }
+    for (int y = 0; y < lines; ++y) range_compress_body<FMT>(a, y, 0, 1, s.data(), nullptr);
 }
 
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void*) {
-    std::vector<float2> s(sh.smem / sizeof(float2) + 1);
-    switch (a.plan.n) {
-        case 768: emu_rc_ct<768>(a, lines, s.data()); return ASARF_OK;
-        case 1024: emu_rc_ct<1024>(a, lines, s.data()); return ASARF_OK;
-        case 1536: emu_rc_ct<1536>(a, lines, s.data()); return ASARF_OK;
-        case 2048: emu_rc_ct<2048>(a, lines, s.data()); return ASARF_OK;
-        case 3072: emu_rc_ct<3072>(a, lines, s.data()); return ASARF_OK;
-        case 4096: emu_rc_ct<4096>(a, lines, s.data()); return ASARF_OK;
-        case 6144: emu_rc_ct<6144>(a, lines, s.data()); return ASARF_OK;
-        case 8192: emu_rc_ct<8192>(a, lines, s.data()); return ASARF_OK;
-        default: break;
-    }
-    for (int y = 0; y < lines; ++y) range_compress_body(a, y, 0, 1, s.data(), nullptr);
+    if (a.format == kRawAsarFbaq4)
+        emu_rc<kRawAsarFbaq4>(a, lines, sh);
+    else
+        emu_rc<kRawErsBytes>(a, lines, sh);
     return ASARF_OK;
 }
 
@@ -90,6 +110,11 @@ int backend_decode(const DecodeArgs& a, long long n, void*) {
     for (long long i = 0; i < n; ++i) decode_item(a, i);
     return ASARF_OK;
 }
+int backend_decode_fbaq(const DecodeFbaqArgs& a, long long n, void*) {
+    for (long long i = 0; i < n; ++i) decode_fbaq_item(a, i);
+    return ASARF_OK;
+}
+
 int backend_img_moments(const ImgMomentsArgs& a, int blocks, void*) {
     std::vector<double> red(12);
     for (int b = 0; b < blocks; ++b) img_moments_body(a, b, 0, 1, red.data());

@@ -443,8 +443,21 @@ static int validate_scene(const asarf_scene* s) {
     if (s->samples_per_line > s->range_size)
         return set_error(ASARF_ERR_INVALID, "samples_per_line %d exceeds range_size %d", s->samples_per_line,
                          s->range_size);
-    if (s->raw_line_bytes < 2 * s->samples_per_line || (s->raw_line_bytes & 1))
-        return set_error(ASARF_ERR_INVALID, "raw_line_bytes must be even and >= 2*samples_per_line");
+    if (s->raw_format == ASARF_RAW_ASAR_FBAQ4) {
+        // samples_per_line samples take 63 per 64-byte block plus one id byte for a partial block
+        const int spl = s->samples_per_line;
+        const long long need = 2 + 64ll * (spl / 63) + (spl % 63 ? spl % 63 + 1 : 0);
+        if (s->raw_line_bytes < need)
+            return set_error(ASARF_ERR_INVALID, "raw_line_bytes %d cannot hold %d FBAQ4 samples (%lld bytes)",
+                             s->raw_line_bytes, spl, need);
+        if (!s->fbaq_i_lut || !s->fbaq_q_lut)
+            return set_error(ASARF_ERR_INVALID, "FBAQ4 records need the instrument reconstruction tables");
+    } else if (s->raw_format == ASARF_RAW_ERS_BYTES) {
+        if (s->raw_line_bytes < 2 * s->samples_per_line || (s->raw_line_bytes & 1))
+            return set_error(ASARF_ERR_INVALID, "raw_line_bytes must be even and >= 2*samples_per_line");
+    } else {
+        return set_error(ASARF_ERR_INVALID, "unknown raw_format %d", s->raw_format);
+    }
     if (s->chirp_samples <= 0 || s->chirp_samples >= s->range_size - 32)
         return set_error(ASARF_ERR_INVALID, "chirp_samples %d incompatible with range_size %d", s->chirp_samples,
                          s->range_size);
@@ -467,6 +480,14 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     p->scene = *scene;
     p->osv.assign(scene->osv, scene->osv + scene->n_osv);
     p->scene.osv = p->osv.data();
+    if (scene->raw_format == ASARF_RAW_ASAR_FBAQ4) {
+        p->fbaq_luts.assign(scene->fbaq_i_lut, scene->fbaq_i_lut + 4096);
+        p->fbaq_luts.insert(p->fbaq_luts.end(), scene->fbaq_q_lut, scene->fbaq_q_lut + 4096);
+        p->scene.fbaq_i_lut = p->fbaq_luts.data();
+        p->scene.fbaq_q_lut = p->fbaq_luts.data() + 4096;
+    } else {
+        p->scene.fbaq_i_lut = p->scene.fbaq_q_lut = nullptr;
+    }
     p->opt = opt;
     const asarf_scene& s = p->scene;
     p->nr = s.range_size;
@@ -621,8 +642,23 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     float2* twN = p->alloc<float2>(p->az_pad);
     float* win = p->alloc<float>(16);
     float* rsl_dev = p->alloc<float>(p->nx);
+    // FBAQ4 records: reconstruction tables permuted to [block id][raw code], and the
+    // statistics partials of every 32-column x kFbaqStatsLines tile
+    const bool fbaq = s.raw_format == ASARF_RAW_ASAR_FBAQ4;
+    const int fb_tiles_x = (p->nr + 31) / 32;
+    const int fb_tiles_y = (p->na + kFbaqStatsLines - 1) / kFbaqStatsLines;
+    const int dc_step0 = p->nr / 32 > 0 ? p->nr / 32 : 1;
+    int fb_span = 1;
+    for (int bx = 0; bx < fb_tiles_x; ++bx) {
+        const int x1 = std::min(bx * 32 + 31, p->nr - 1);
+        fb_span = std::max(fb_span, x1 / dc_step0 - (bx * 32) / dc_step0 + 1);
+    }
+    const int fb_slots = 6 + 9 * fb_span;
+    float* lut_dev = fbaq ? p->alloc<float>(2 * 4096) : nullptr;
+    double* part_dev = fbaq ? p->alloc<double>(static_cast<size_t>(fb_tiles_y) * fb_tiles_x * fb_slots) : nullptr;
+    FloatStatAccum* facc_dev = fbaq ? p->alloc<FloatStatAccum>(1) : nullptr;
     if (!p->bufA || !p->bufB || !p->acc || !p->state || !p->raw_dev || !p->swst_dev || !p->out_dev || !rc_tw ||
-        !p->rc_mf || !tw1 || !drev1 || !tw2 || !drev2 || !twN || !win || !rsl_dev) {
+        !p->rc_mf || !tw1 || !drev1 || !tw2 || !drev2 || !twN || !win || !rsl_dev || (fbaq && (!lut_dev || !part_dev || !facc_dev))) {
         const size_t need = p->bytes;
         delete p;
         return set_error(ASARF_ERR_NOMEM, "device allocation failed (plan needs about %zu MB)",
@@ -642,6 +678,15 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     rc |= mem_h2d(twN, p->fN.tw.data(), sizeof(float2) * p->az_pad, nullptr);
     rc |= mem_h2d(win, w16, sizeof(w16), nullptr);
     rc |= mem_h2d(rsl_dev, rsl.data(), sizeof(float) * p->nx, nullptr);
+    if (fbaq) {
+        std::vector<float> lut(2 * 4096);
+        for (int id = 0; id < 256; ++id)
+            for (int code = 0; code < 16; ++code) {
+                lut[16 * id + code] = s.fbaq_i_lut[fbaq4_index(id, code)];
+                lut[4096 + 16 * id + code] = s.fbaq_q_lut[fbaq4_index(id, code)];
+            }
+        rc |= mem_h2d(lut_dev, lut.data(), sizeof(float) * lut.size(), nullptr);
+    }
     rc |= mem_zero(p->state, sizeof(FocusState), nullptr);
     rc |= stream_sync(nullptr);
     if (rc) {
@@ -669,6 +714,16 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     st.lines_per_cta = kStatsMaxLines / 4;
     st.acc = p->acc;
     p->stats_gy = (p->na + st.lines_per_cta - 1) / st.lines_per_cta;
+    if (fbaq) {
+        st.lut_i = lut_dev;
+        st.lut_q = lut_dev + 4096;
+        st.part = part_dev;
+        st.facc = facc_dev;
+        st.tiles_x = fb_tiles_x;
+        st.span = fb_span;
+        st.part_slots = fb_slots;
+        p->stats_gy = fb_tiles_y;
+    }
 
 
     FinalizeArgs& fin = p->a_fin;
@@ -686,6 +741,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     fin.lines_before = s.lines_before;
     fin.lines_after = s.lines_after;
     fin.max_aperture = max_ap;
+    fin.facc = facc_dev;
     fin.dc_given = opt.dc_poly_given ? 1 : 0;
     for (int k = 0; k < 3; ++k) fin.dc_in[k] = opt.dc_poly[k];
     for (int v = 0; v < 2; ++v) {
@@ -705,6 +761,11 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     r.nk = p->nk;
     r.out = p->bufA;
     r.out_pitch = p->pitch;
+    r.format = s.raw_format;
+    if (fbaq) {
+        r.lut_i = lut_dev;
+        r.lut_q = lut_dev + 4096;
+    }
     const int rc_elems = n_ctr ? ct_smem_elems_of(p->rc_len) : p->rc_len;  // compile-time lengths: padded tile
     p->raw_smem_offset = static_cast<int>((sizeof(float2) * static_cast<size_t>(rc_elems) + 127) / 128 * 128);
     p->sh_rc = {512, static_cast<size_t>(p->raw_smem_offset) + (2 * static_cast<size_t>(s.samples_per_line) + 15) / 16 * 16};
@@ -851,7 +912,9 @@ static const char* const kKernelNames[kKernelsPerRun] = {"raw_stats", "finalize"
 int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int32_t min_swst, float* d_out,
                 void* stream) {
     if (!p || !d_raw || (!d_out && !p->skip_tail)) return set_error(ASARF_ERR_INVALID, "focus: null argument");
-    if (reinterpret_cast<uintptr_t>(d_raw) & 1) return set_error(ASARF_ERR_INVALID, "raw buffer must be 2-byte aligned");
+    const bool fbaq = p->scene.raw_format == ASARF_RAW_ASAR_FBAQ4;
+    if (!fbaq && (reinterpret_cast<uintptr_t>(d_raw) & 1))
+        return set_error(ASARF_ERR_INVALID, "raw buffer must be 2-byte aligned");
     void** ev = nullptr;
     if (p->timing_used < p->timing_slots) {
         ev = &p->events[static_cast<size_t>(p->timing_used) * (kKernelsPerRun + 1)];
@@ -869,8 +932,13 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     st.swst = d_swst;
     st.min_swst = min_swst;
     mark();
-    const int stats_gx = raw_stats_grid_x(st, d_raw);
-    rc = backend_raw_stats(st, stats_gx, p->stats_gy, stream);
+    if (fbaq) {
+        rc = backend_raw_stats_fbaq(st, st.tiles_x, p->stats_gy, stream);
+        if (!rc) rc = backend_stats_fold(st, p->stats_gy, stream);
+    } else {
+        const int stats_gx = raw_stats_grid_x(st, d_raw);
+        rc = backend_raw_stats(st, stats_gx, p->stats_gy, stream);
+    }
     if (rc) return rc;
     mark();
     rc = backend_finalize(p->a_fin, stream);
@@ -880,7 +948,7 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     r.swst = d_swst;
     r.min_swst = min_swst;
     const bool aligned = (reinterpret_cast<uintptr_t>(d_raw) % 16 == 0) && (p->scene.raw_line_bytes % 16 == 0);
-    r.bulk_bytes = (p->use_tma && aligned) ? (2 * p->scene.samples_per_line) / 16 * 16 : 0;
+    r.bulk_bytes = (p->use_tma && aligned && !fbaq) ? (2 * p->scene.samples_per_line) / 16 * 16 : 0;
     r.raw_smem_offset = p->raw_smem_offset;
     mark();
     rc = backend_range_compress(r, p->na, p->sh_rc, stream);

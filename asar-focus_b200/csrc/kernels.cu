@@ -24,12 +24,22 @@ __global__ void __launch_bounds__(kStatsCols, 3) k_raw_stats(RawStatsArgs a) {
     raw_stats_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, &sm);
 }
 
+__global__ void __launch_bounds__(32 * kFbaqStatsWarps) k_raw_stats_fbaq(RawStatsArgs a) {
+    __shared__ FbaqStatsSmem sm;
+    raw_stats_fbaq_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, &sm);
+}
+
+__global__ void __launch_bounds__(1024) k_stats_fold(RawStatsArgs a, int tiles_y) {
+    stats_fold_body(a, tiles_y, threadIdx.x, blockDim.x);
+}
+
 __global__ void k_finalize(FinalizeArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) finalize_body(a);
 }
 
 // One raw line per block; with bulk_bytes > 0 thread 0 fetches the line with one bulk copy
 // into shared memory (the sub-16-byte tail with plain loads) while the others wait.
+template <int FMT>
 __global__ void __launch_bounds__(512) k_range_compress(RangeCompressArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_rc_raw[];
     float2* s = reinterpret_cast<float2*>(smem_rc_raw);
@@ -49,11 +59,11 @@ __global__ void __launch_bounds__(512) k_range_compress(RangeCompressArgs a) {
         mbar_wait(&bar, 0, &const_cast<FocusState*>(a.state)->errors);
         line = buf;
     }
-    range_compress_body(a, blockIdx.x, threadIdx.x, blockDim.x, s, line);
+    range_compress_body<FMT>(a, blockIdx.x, threadIdx.x, blockDim.x, s, line);
 }
 
 // Compile-time-scheduled variant (L in kCtLengths).
-template <int L>
+template <int L, int FMT>
 __global__ void __launch_bounds__(CtSchedule<L>::nthr, 2) k_range_compress_ct(RangeCompressArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_rcc_raw[];
     float2* s = reinterpret_cast<float2*>(smem_rcc_raw);
@@ -73,7 +83,7 @@ __global__ void __launch_bounds__(CtSchedule<L>::nthr, 2) k_range_compress_ct(Ra
         mbar_wait(&bar, 0, &const_cast<FocusState*>(a.state)->errors);
         line = buf;
     }
-    range_compress_ct_body<L>(a, blockIdx.x, threadIdx.x, s, line);
+    range_compress_ct_body<L, FMT>(a, blockIdx.x, threadIdx.x, s, line);
 }
 
 // Strided azimuth pass: the [n1][xt] tile (rows r*n2 + b) arrives by 3-D TMA boxes.
@@ -198,30 +208,46 @@ int backend_finalize(const FinalizeArgs& a, void* stream) {
     return check_launch("finalize");
 }
 
-template <int L>
+int backend_raw_stats_fbaq(const RawStatsArgs& a, int gx, int gy, void* stream) {
+    k_raw_stats_fbaq<<<dim3(gx, gy), 32 * kFbaqStatsWarps, 0, S(stream)>>>(a);
+    return check_launch("raw_stats_fbaq");
+}
+
+int backend_stats_fold(const RawStatsArgs& a, int tiles_y, void* stream) {
+    k_stats_fold<<<1, 1024, 0, S(stream)>>>(a, tiles_y);
+    return check_launch("stats_fold");
+}
+
+template <int L, int FMT>
 static int launch_rc_ct(const RangeCompressArgs& a, int lines, size_t smem, void* stream) {
-    int rc = ensure_smem(k_range_compress_ct<L>, smem, "range_compress");
+    int rc = ensure_smem(k_range_compress_ct<L, FMT>, smem, "range_compress");
     if (rc) return rc;
-    k_range_compress_ct<L><<<lines, CtSchedule<L>::nthr, smem, S(stream)>>>(a);
+    k_range_compress_ct<L, FMT><<<lines, CtSchedule<L>::nthr, smem, S(stream)>>>(a);
+    return check_launch("range_compress");
+}
+
+template <int FMT>
+static int launch_rc(const RangeCompressArgs& a, int lines, LaunchShape sh, void* stream) {
+    switch (a.plan.n) {
+        case 768: return launch_rc_ct<768, FMT>(a, lines, sh.smem, stream);
+        case 1024: return launch_rc_ct<1024, FMT>(a, lines, sh.smem, stream);
+        case 1536: return launch_rc_ct<1536, FMT>(a, lines, sh.smem, stream);
+        case 2048: return launch_rc_ct<2048, FMT>(a, lines, sh.smem, stream);
+        case 3072: return launch_rc_ct<3072, FMT>(a, lines, sh.smem, stream);
+        case 4096: return launch_rc_ct<4096, FMT>(a, lines, sh.smem, stream);
+        case 6144: return launch_rc_ct<6144, FMT>(a, lines, sh.smem, stream);
+        case 8192: return launch_rc_ct<8192, FMT>(a, lines, sh.smem, stream);
+        default: break;
+    }
+    int rc = ensure_smem(k_range_compress<FMT>, sh.smem, "range_compress");
+    if (rc) return rc;
+    k_range_compress<FMT><<<lines, sh.threads, sh.smem, S(stream)>>>(a);
     return check_launch("range_compress");
 }
 
 int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh, void* stream) {
-    switch (a.plan.n) {
-        case 768: return launch_rc_ct<768>(a, lines, sh.smem, stream);
-        case 1024: return launch_rc_ct<1024>(a, lines, sh.smem, stream);
-        case 1536: return launch_rc_ct<1536>(a, lines, sh.smem, stream);
-        case 2048: return launch_rc_ct<2048>(a, lines, sh.smem, stream);
-        case 3072: return launch_rc_ct<3072>(a, lines, sh.smem, stream);
-        case 4096: return launch_rc_ct<4096>(a, lines, sh.smem, stream);
-        case 6144: return launch_rc_ct<6144>(a, lines, sh.smem, stream);
-        case 8192: return launch_rc_ct<8192>(a, lines, sh.smem, stream);
-        default: break;
-    }
-    int rc = ensure_smem(k_range_compress, sh.smem, "range_compress");
-    if (rc) return rc;
-    k_range_compress<<<lines, sh.threads, sh.smem, S(stream)>>>(a);
-    return check_launch("range_compress");
+    if (a.format == kRawAsarFbaq4) return launch_rc<kRawAsarFbaq4>(a, lines, sh, stream);
+    return launch_rc<kRawErsBytes>(a, lines, sh, stream);
 }
 
 static CUtensorMap tmap_or_zero(const void* tmap) {
@@ -286,6 +312,10 @@ int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err,
 int backend_decode(const DecodeArgs& a, long long n, void* stream) {
     k_items<DecodeArgs, decode_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);
     return check_launch("decode");
+}
+int backend_decode_fbaq(const DecodeFbaqArgs& a, long long n, void* stream) {
+    k_items<DecodeFbaqArgs, decode_fbaq_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);
+    return check_launch("decode_fbaq");
 }
 int backend_img_moments(const ImgMomentsArgs& a, int blocks, void* stream) {
     k_img_moments<<<blocks, 256, 0, S(stream)>>>(a);

@@ -21,6 +21,24 @@ struct StatAccum {
     unsigned long long lag[kMaxDcBlocks][9];
 };
 
+// ASAR FBAQ4 records: the same sums over the decoded float samples, in FP64, written (not
+// accumulated) by the fold of the per-tile partials in a fixed order, so reproducible.
+struct FloatStatAccum {
+    double mom[6];
+    double lag[kMaxDcBlocks][9];
+};
+
+// Raw record formats of the fused path.
+enum RawFormat : int {
+    kRawErsBytes = 0,   // ERS byte I/Q pairs, SWST shift 4 samples per code step
+    kRawAsarFbaq4 = 1,  // ENVISAT ASAR FBAQ4 blocks, SWST shift 1 sample per code step
+};
+
+// FBAQ4 statistics tiles: 32 columns (one per lane) x kFbaqStatsLines lines, split over the
+// 8 warps of a block.
+constexpr int kFbaqStatsLines = 2048;
+constexpr int kFbaqStatsWarps = 8;
+
 // Per-column-independent output of the statistics finalisation, read by later kernels.
 struct FocusState {
     float dc_i, dc_q, gain, sin_c, cos_c;  // IQ correction as the reference applies it
@@ -58,6 +76,7 @@ struct FinalizeArgs {
     double prf;
     // results window inputs (CalcResultsWindow)
     int lines_before, lines_after, max_aperture;
+    const FloatStatAccum* facc;  // FBAQ4 records: read these FP64 sums instead of acc
     int dc_given;            // use dc_in instead of the estimate
     double dc_in[3];
     int first_line[kNumTailVariants];
@@ -76,6 +95,14 @@ struct RawStatsArgs {
     int quad;             // 4-column units (raw base and line stride 8-byte aligned)
     int gpb;              // 4-column groups per Doppler block: ceil(dc_step / 4)
     StatAccum* acc;
+    // ASAR FBAQ4 records (k_raw_stats_fbaq): FP64 partial sums of each 32-column tile
+    const float* lut_i;   // [256 block ids][16 raw codes]
+    const float* lut_q;
+    double* part;         // [tiles_y][tiles_x][part_slots]
+    FloatStatAccum* facc; // folded sums
+    int tiles_x;          // ceil(nr / 32)
+    int span;             // Doppler blocks one 32-column tile can touch
+    int part_slots;       // 6 moments + 9 lag sums per touched Doppler block
 };
 
 struct RangeCompressArgs {
@@ -95,6 +122,9 @@ struct RangeCompressArgs {
     long long out_pitch;
     int bulk_bytes;       // raw bytes per line fetched by one bulk copy (multiple of 16; 0 = plain loads)
     int raw_smem_offset;  // byte offset of the raw-line buffer in shared memory
+    int format;           // RawFormat of the records
+    const float* lut_i;   // ASAR FBAQ4 records: [256 block ids][16 raw codes]
+    const float* lut_q;
 };
 
 struct AzStridedArgs {
@@ -177,6 +207,19 @@ struct DecodeArgs {
     int min_swst;
     float2* img;
     long long stride;   // complex elements per image row
+};
+
+// ASAR FBAQ4 records -> complex rows, NaN where no sample (ConvertAsarImBlocksToComplex)
+struct DecodeFbaqArgs {
+    const uint8_t* raw;
+    long long line_bytes;   // record stride: 2 length bytes + block data
+    int lines, nr;
+    const uint16_t* swst;
+    int min_swst;
+    const float* lut_i;     // 4096 entries, [level][block id] order of the instrument file
+    const float* lut_q;
+    float2* img;
+    long long stride;
 };
 
 // NaN-aware moment partials of rows [row0, row0 + rows) per block: data region x < x_size

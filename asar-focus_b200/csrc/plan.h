@@ -28,6 +28,7 @@ using asarf::stream_destroy;
 struct asarf_plan {
     asarf_scene scene{};
     std::vector<asarf_osv> osv;
+    std::vector<float> fbaq_luts;  // the scene's FBAQ4 tables (I then Q), owned copy
     asarf_options opt{};
     asarf_dims dims{};
     int nr = 0, na = 0, nc = 0, nk = 0, nx = 0;

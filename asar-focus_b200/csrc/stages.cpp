@@ -88,6 +88,30 @@ int asarf_convert_ers_samples(const uint8_t* d_raw, int32_t raw_line_bytes, int3
     return stream_sync(stream);
 }
 
+int asarf_convert_asar_blocks(const uint8_t* d_raw, int32_t record_bytes, int32_t records, const uint16_t* d_swst,
+                              int32_t min_swst, const float* d_lut_i, const float* d_lut_q, void* d_img,
+                              int64_t img_stride, int32_t range_size, void* stream) {
+    if (!d_raw || !d_img || !d_lut_i || !d_lut_q || records <= 0 || record_bytes < 2 || range_size <= 0 ||
+        img_stride < range_size)
+        return set_error(ASARF_ERR_INVALID, "convert_asar_blocks: bad arguments");
+    DecodeFbaqArgs a{};
+    a.raw = d_raw;
+    a.line_bytes = record_bytes;
+    a.lines = records;
+    a.nr = range_size;
+    a.swst = d_swst;
+    a.min_swst = min_swst;
+    a.lut_i = d_lut_i;
+    a.lut_q = d_lut_q;
+    a.img = static_cast<float2*>(d_img);
+    a.stride = img_stride;
+    int rc = backend_decode_fbaq(a, static_cast<long long>(records) * range_size, stream);
+    if (rc) return rc;
+    return stream_sync(stream);
+}
+
+int32_t asarf_fbaq4_index(int32_t block, int32_t code) { return fbaq4_index(block, code); }
+
 int asarf_raw_data_correction(void* d_img, int32_t x_size, int32_t y_size, int32_t x_stride, int32_t y_stride,
                               int64_t n_total_samples, asarf_iq_results* results, void* stream) {
     if (!d_img || !results || x_size <= 0 || y_size <= 0 || x_stride < x_size || y_stride < y_size)

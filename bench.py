@@ -151,11 +151,12 @@ def _barrier(world: int):
 
 def _describe(sc) -> str:
     kind = "ASAR IM-like" if sc.bits == 8 else "ERS-like"
+    fmt = "FBAQ4 records (synthetic tables)" if sc.raw_format == "fbaq4" else f"{sc.bits}-bit I/Q"
     dc = f"Doppler {sc.dc_coeffs[0]:+.0f} Hz + range terms" if sc.dc_kind == "poly" else \
         f"Doppler drifting +-{sc.dc_drift:.0f} Hz along azimuth"
     grid = f"{sc.grid[0]}x{sc.grid[1]} point grid"
     vr = "Vr from the orbit state vectors" if sc.vr_given is None else f"Vr {sc.vr_given:.0f} m/s"
-    return f"{kind} {sc.range_size} range x {sc.azimuth_size} azimuth, {sc.bits}-bit I/Q, {grid}, {dc}, {vr}"
+    return f"{kind} {sc.range_size} range x {sc.azimuth_size} azimuth, {fmt}, {grid}, {dc}, {vr}"
 
 
 def make_scene(workload: str, seed: int):
@@ -166,10 +167,10 @@ def make_scene(workload: str, seed: int):
 def algorithmic_bytes(sc, dims: dict, res: dict) -> dict:
     """Minimal HBM bytes each kernel must move (inputs read once, outputs written once,
     no halo, no padding rows), per launch."""
-    na, spl = sc.azimuth_size, sc.samples_per_line
+    na = sc.azimuth_size
     nk, az = dims["nk"], dims["az_pad"]
     nx = dims["slc_cols"]
-    raw = na * 2 * spl
+    raw = na * sc.raw_line_bytes
     nl = res["n_lines"]
     out = res["out_rows"] * res["out_cols"] * 4
     return {"raw_stats": raw, "finalize": 0, "range_compress": raw + na * nk * 8,
@@ -180,11 +181,11 @@ def algorithmic_bytes(sc, dims: dict, res: dict) -> dict:
 def pipeline_bytes(sc, dims: dict, res: dict) -> float:
     """Algorithmic bytes of the whole scene: raw read twice, two complex round trips,
     multilooked float round trip, ground-range output write (unpadded sizes)."""
-    na, nr = sc.azimuth_size, sc.range_size
+    na = sc.azimuth_size
     nk = dims["nk"]
     L = 5.0
     ng = res["out_cols"]
-    return na * 2 * nr * 2 + 32 * nk * na + 8 * nk * na / L + 4 * ng * na / L
+    return na * sc.raw_line_bytes * 2 + 32 * nk * na + 8 * nk * na / L + 4 * ng * na / L
 
 
 def _traffic_from_profiles(kernel: str, workload: str):

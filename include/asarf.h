@@ -34,13 +34,19 @@ typedef struct asarf_osv {
     double vel[3];
 } asarf_osv;
 
+/* Raw record formats (asarf_scene.raw_format). */
+#define ASARF_RAW_ERS_BYTES 0   /* ERS byte I/Q pairs (ConvertErsImSamplesToComplex) */
+#define ASARF_RAW_ASAR_FBAQ4 1  /* ENVISAT ASAR FBAQ4 blocks (ConvertAsarImBlocksToComplex) */
+
 /* Scene description: the fields of SARMetadata (sar/sar_metadata.h:57-88) that the
- * focusing path reads, plus the raw record layout of the ERS byte-I/Q decoder. */
+ * focusing path reads, plus the raw record layout of the decoder. */
 typedef struct asarf_scene {
-    int32_t range_size;        /* XSize of the decoded image: samples_per_line + 4*(max_swst-min_swst) */
+    int32_t range_size;        /* XSize of the decoded image: samples_per_line + k*(max_swst-min_swst),
+                                  k = 4 (ERS) or 1 (ASAR) */
     int32_t azimuth_size;      /* YSize: number of echo lines */
-    int32_t samples_per_line;  /* I/Q byte pairs per raw record */
-    int32_t raw_line_bytes;    /* byte stride of raw records (even, >= 2*samples_per_line) */
+    int32_t samples_per_line;  /* ERS: I/Q byte pairs per raw record; ASAR: the most samples of any record */
+    int32_t raw_line_bytes;    /* byte stride of raw records; ERS: even, >= 2*samples_per_line;
+                                  ASAR: 2 length bytes + block data (RawSampleMeasurements::single_entry_length + 2) */
     int64_t total_raw_samples; /* CorrectionParams::n_total_samples (sar/iq_correction.cuh:22-25) */
     /* ChirpInfo (sar/sar_metadata.h:34-44) */
     double range_sampling_rate;
@@ -66,6 +72,12 @@ typedef struct asarf_scene {
     double center_point[3];    /* ECEF scene centre, initial guess of every geolocation */
     int32_t lines_before;      /* lines cached before sensing start (CalcResultsWindow) */
     int32_t lines_after;       /* lines cached after sensing stop */
+    int32_t raw_format;        /* ASARF_RAW_ERS_BYTES (0) or ASARF_RAW_ASAR_FBAQ4 */
+    /* ASAR FBAQ4: the instrument file's reconstruction tables (InstrumentFile fbp.i_LUT_fbaq4 /
+     * q_LUT_fbaq4, envisat_format/include/envisat_aux_file.h:145-148), 4096 floats each at
+     * index 256 * level + block id; read at plan creation only */
+    const float* fbaq_i_lut;
+    const float* fbaq_q_lut;
 } asarf_scene;
 
 /* Options of the fused plan. */
@@ -119,7 +131,8 @@ int asarf_plan_dims(const asarf_plan* plan, asarf_dims* dims);
 
 /* Focus one scene from device-resident raw bytes to the detected ground-range image
  * (float [out_rows][out_cols_max], row pitch out_cols_max).  Replaces main.cc:233-327:
- * ConvertErsImSamplesToComplex + RawDataCorrection + ZeroNaNs + CalculateDopplerCentroid +
+ * ConvertErsImSamplesToComplex (FBAQ4 records: ConvertAsarImBlocksToComplex) +
+ * RawDataCorrection + ZeroNaNs + CalculateDopplerCentroid +
  * RangeCompression + RangeDopplerAlgorithm + SubsetResultsAndReassembleMeta +
  * AzimuthMultiLook + RangeSpreadingLossCorrection + SlantRangeToGroundRangeInterpolation.
  * swst may be NULL (all lines start at range sample 0). Asynchronous on `stream`. */
@@ -315,6 +328,18 @@ typedef struct asarf_rda_params {
 int asarf_convert_ers_samples(const uint8_t* d_raw, int32_t raw_line_bytes, int32_t samples_per_line, int32_t lines,
                               const uint16_t* d_swst, int32_t min_swst, void* d_img, int64_t img_stride,
                               int32_t range_size, void* stream);
+/* ConvertAsarImBlocksToComplexKernel (envisat_format/src/envisat_format_kernels.cu:160-209) with
+ * the NaN pre-fill of main_flow.cc:537-540, on device buffers: FBAQ4 records of `record_bytes`
+ * bytes (2-byte little-endian block-data length, then 64-byte blocks of a block id and 63
+ * codewords) -> complex rows of `range_size` samples, record y shifted right by
+ * swst[y] - min_swst (d_swst may be NULL), samples the record does not hold NaN.  d_lut_i /
+ * d_lut_q: the 4096-entry reconstruction tables on the device, instrument-file order. */
+int asarf_convert_asar_blocks(const uint8_t* d_raw, int32_t record_bytes, int32_t records, const uint16_t* d_swst,
+                              int32_t min_swst, const float* d_lut_i, const float* d_lut_q, void* d_img,
+                              int64_t img_stride, int32_t range_size, void* stream);
+/* Fbaq4Index (envisat_format/include/envisat_parse_util.h:21): reconstruction-table index of
+ * the 4-bit code `code` in a block with block id `block` (256 * level + block). */
+int32_t asarf_fbaq4_index(int32_t block, int32_t code);
 /* RawDataCorrection (sar/iq_correction.cu:188-274): means and deviations over the data
  * block (NaN samples skipped, divided by n_total_samples; <= 0 means x_size*y_size), then
  * DC, gain and phase correction applied over x < x_stride, y < y_size with the gain and

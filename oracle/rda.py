@@ -101,6 +101,59 @@ def decode_ers(raw: np.ndarray, samples_per_line: int, swst: np.ndarray | None, 
     return out
 
 
+def fbaq4_index(block, code):
+    """Fbaq4IndexCalc (envisat_format/include/envisat_parse_util.cuh:75-84): table index
+    256 * level + block id, level = 15 - code for codes above 7, else 8 + code."""
+    code = np.asarray(code, dtype=np.int64)
+    return 256 * np.where(code > 7, 15 - code, 8 + code) + np.asarray(block, dtype=np.int64)
+
+
+def decode_asar_fbaq(raw: np.ndarray, swst: np.ndarray | None, range_size: int, i_lut: np.ndarray,
+                     q_lut: np.ndarray, chunk: int = 1024) -> np.ndarray:
+    """ConvertAsarImBlocksToComplexKernel (envisat_format/src/envisat_format_kernels.cu:160-209)
+    after the NaN pre-fill (main_flow.cc:537-540).  Record y (raw[y], its byte stride the record
+    size): 2-byte little-endian block-data length L, then per byte j < L of the block data that is
+    not a block id (j % 64 != 0) the sample j - (j // 64 + 1), shifted right by swst[y] - min(swst),
+    I from the high nibble and Q from the low nibble of the byte through the tables.  The
+    reference indexes the output flat (y * range_size + sample) without a range check, so a
+    record longer than range_size would continue into the next row; that is kept here (writes
+    past the last row are dropped).  Bit-exact: table lookups only."""
+    na, rec = raw.shape
+    out_re = np.full(na * range_size, np.nan, dtype=np.float32)
+    out_im = np.full(na * range_size, np.nan, dtype=np.float32)
+    sw = np.zeros(na, dtype=np.int64) if swst is None else np.asarray(swst, dtype=np.int64)
+    off = sw - sw.min()
+    j = np.arange(rec - 2, dtype=np.int64)
+    b = j // 64
+    not_id = (j % 64) != 0
+    for y0 in range(0, na, chunk):
+        y1 = min(na, y0 + chunk)
+        r8 = raw[y0:y1].astype(np.int64)
+        length = r8[:, 0] | (r8[:, 1] << 8)
+        valid = (j[None, :] < length[:, None]) & not_id[None, :]
+        bid = r8[:, 2 + 64 * b]
+        cw = r8[:, 2 + j]
+        ii = fbaq4_index(bid, cw >> 4)
+        qi = fbaq4_index(bid, cw & 15)
+        valid &= (ii < i_lut.shape[0]) & (qi < q_lut.shape[0])
+        flat = (np.arange(y0, y1)[:, None] * range_size + j[None, :] - (b[None, :] + 1) + off[y0:y1, None])
+        keep = valid & (flat < na * range_size)
+        out_re[flat[keep]] = i_lut[ii[keep]]
+        out_im[flat[keep]] = q_lut[qi[keep]]
+    out = np.empty(na * range_size, dtype=np.complex64)
+    out.real = out_re
+    out.imag = out_im
+    return out.reshape(na, range_size)
+
+
+def decode(raw: np.ndarray, scene: dict) -> np.ndarray:
+    """The decoder of the scene's record format (main_flow.cc:530-583)."""
+    if scene.get("raw_format", "ers") == "fbaq4":
+        ti, tq = scene["fbaq_tables"]
+        return decode_asar_fbaq(raw, scene.get("swst"), scene["range_size"], ti, tq)
+    return decode_ers(raw, scene["samples_per_line"], scene.get("swst"), scene["range_size"])
+
+
 def pad_image(data: np.ndarray, rg_pad: int, az_pad: int) -> np.ndarray:
     """InitPadded + ZeroMemory + cudaMemcpy2D of the decoded block (main.cc:233-238)."""
     na, nr = data.shape
@@ -448,7 +501,7 @@ def _range_doppler_image(raw: np.ndarray, scene: dict, ref_compat: bool = True):
     na = scene["azimuth_size"]
     nc = scene["chirp_samples"]
     rg_pad, az_pad = geo.reference_padding(nr, nc, na)
-    img = pad_image(decode_ers(raw, scene["samples_per_line"], scene.get("swst"), nr), rg_pad, az_pad)
+    img = pad_image(decode(raw, scene), rg_pad, az_pad)
     raw_data_correction(img, nr, na, scene["total_raw_samples"], ref_compat)
     zero_nans(img)
     osv = [geo.Osv(*o) for o in scene["osv"]]
@@ -523,13 +576,13 @@ def focus_strip(raw: np.ndarray, scene: dict, block: int, overlap: int, ref_comp
 
 
 def focus(raw: np.ndarray, scene: dict, ref_compat: bool = True, keep_intermediate: bool = False) -> FocusResult:
-    """main.cc:233-327 for an ERS-style byte-I/Q scene described by ``scene`` (see
-    ``asarf.scene.Scene.to_dict``)."""
+    """main.cc:233-327 for a scene described by ``scene`` (see ``asarf.scene.Scene.to_dict``):
+    ERS byte-I/Q or ASAR FBAQ4 records."""
     nr = scene["range_size"]
     na = scene["azimuth_size"]
     nc = scene["chirp_samples"]
     rg_pad, az_pad = geo.reference_padding(nr, nc, na)
-    data = decode_ers(raw, scene["samples_per_line"], scene.get("swst"), nr)
+    data = decode(raw, scene)
     img = pad_image(data, rg_pad, az_pad)
     del data
     iq = raw_data_correction(img, nr, na, scene["total_raw_samples"], ref_compat)

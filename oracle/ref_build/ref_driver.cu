@@ -197,7 +197,11 @@ int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_ra
         cufftComplex* d_parsed = nullptr;
         CHECK_CUDA_ERR(cudaMalloc(&d_parsed, sizeof(cufftComplex) * static_cast<size_t>(nr) * na));
         alus::cuda::algorithm::Fill(d_parsed, static_cast<size_t>(nr) * na, cufftComplex{NAN, NAN});
-        if (d_raw) {
+        if (s->raw_format == ASARF_RAW_ASAR_FBAQ4) {
+            // ASA_IM0 branch of ConvertRawSampleSetsToComplex (main_flow.cc:566-575), host records
+            alus::asar::envformat::ConvertAsarImBlocksToComplex(h_raw, s->raw_line_bytes, na, swst.data(), min_swst,
+                                                               d_parsed, nr, s->fbaq_i_lut, s->fbaq_q_lut, 4096);
+        } else if (d_raw) {
             const int x_size = 11232;  // ers::highrate::MEASUREMENT_DATA_SIZE_BYTES, as the wrapper sizes its grid
             dim3 block(16, 16), grid((x_size + 15) / 16, (na + 15) / 16);
             alus::asar::envformat::ConvertErsImSamplesToComplexKernel<<<grid, block>>>(
@@ -314,6 +318,28 @@ int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_ra
     } catch (const std::exception& e) {
         std::snprintf(o->error, sizeof(o->error), "%s", e.what());
         return -2;
+    }
+}
+
+// The reference's ASAR FBAQ4 decode alone: NaN-filled device image (main_flow.cc:537-540),
+// ConvertAsarImBlocksToComplex from host records and tables, copied back as [records][range_size].
+int ref_convert_asar(const uint8_t* h_raw, int32_t record_bytes, int32_t records, const uint16_t* h_swst,
+                     const float* i_lut, const float* q_lut, int32_t range_size, float* h_out) {
+    try {
+        std::vector<uint16_t> swst(records, 0);
+        if (h_swst) swst.assign(h_swst, h_swst + records);
+        const uint16_t min_swst = *std::min_element(swst.begin(), swst.end());
+        const size_t n = static_cast<size_t>(range_size) * records;
+        cufftComplex* d = nullptr;
+        CHECK_CUDA_ERR(cudaMalloc(&d, sizeof(cufftComplex) * n));
+        alus::cuda::algorithm::Fill(d, n, cufftComplex{NAN, NAN});
+        alus::asar::envformat::ConvertAsarImBlocksToComplex(h_raw, record_bytes, records, swst.data(), min_swst, d,
+                                                           range_size, i_lut, q_lut, 4096);
+        CHECK_CUDA_ERR(cudaMemcpy(h_out, d, sizeof(cufftComplex) * n, cudaMemcpyDeviceToHost));
+        CHECK_CUDA_ERR(cudaFree(d));
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
     }
 }
 

@@ -42,8 +42,31 @@ def load(path: Path = REF_LIB):
         f.restype = C.c_int
         f.argtypes = [C.c_void_p, C.POINTER(C.c_double * 3), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                       C.POINTER(RefOutputs), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        if hasattr(lib, "ref_convert_asar"):
+            g = lib.ref_convert_asar
+            g.restype = C.c_int
+            g.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                          C.c_void_p]
         _libs[path] = lib
     return _libs[path]
+
+
+def ref_convert_asar(raw: np.ndarray, swst, i_lut: np.ndarray, q_lut: np.ndarray, range_size: int,
+                     lib_path: Path = REF_LIB) -> np.ndarray:
+    """The reference's ConvertAsarImBlocksToComplex on host FBAQ4 records (NaN pre-filled
+    image, main_flow.cc:537-540): complex64 [records, range_size]."""
+    lib = load(lib_path)
+    raw = np.ascontiguousarray(raw, dtype=np.uint8)
+    na, rec = raw.shape
+    sw = None if swst is None else np.ascontiguousarray(swst, dtype=np.uint16)
+    ti = np.ascontiguousarray(i_lut, dtype=np.float32)
+    tq = np.ascontiguousarray(q_lut, dtype=np.float32)
+    out = np.empty((na, range_size), dtype=np.complex64)
+    rc = lib.ref_convert_asar(raw.ctypes.data, rec, na, None if sw is None else sw.ctypes.data, ti.ctypes.data,
+                              tq.ctypes.data, range_size, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reference ConvertAsarImBlocksToComplex failed")
+    return out
 
 
 def ref_focus(scene_c, vr_poly, raw: np.ndarray, swst=None, dumps: bool = False, out_capacity: int | None = None,
