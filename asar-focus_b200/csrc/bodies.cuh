@@ -424,6 +424,7 @@ ASARF_HD ASARF_INLINE bool fbaq_sample(const uint8_t* rec, int len, int r, const
 // block in lane order), and the tile's partials are written, not accumulated: the fold sums
 // them in a fixed order, so the statistics do not depend on scheduling.
 constexpr int kFbaqSums = 15;  // 6 moments + 9 lag sums
+constexpr int kFoldTree = 256; // leaves of the moment tree of the fold (column tiles wrap onto them)
 struct FbaqStatsSmem {
     int off[kFbaqStatsLines + 1];  // SWST shift of the tile's lines (and the line before)
     int len[kFbaqStatsLines + 1];  // usable block-data bytes of those records
@@ -457,24 +458,27 @@ ASARF_HD ASARF_INLINE void raw_stats_fbaq_body(const RawStatsArgs& a, int bx, in
             for (int yb = start; yb < wy1; yb += kStatsBatch) {
                 float iv[kStatsBatch], qv[kStatsBatch];
                 bool f[kStatsBatch];
+                // branch-free batch: an absent sample reads byte 0 of its record's block data
+                // (inside the record: every record holds at least one block byte) and is masked
 #pragma unroll
                 for (int u = 0; u < kStatsBatch; ++u) {
-                    const int y = yb + u;
-                    f[u] = false;
-                    iv[u] = 0.0f;
-                    qv[u] = 0.0f;
-                    if (y < wy1) {
-                        const int r = x - sm->off[y - ys];
-                        if (r >= 0)
-                            f[u] = fbaq_sample(a.raw + static_cast<long long>(y) * a.line_bytes, sm->len[y - ys], r,
-                                               d63, a.lut_i, a.lut_q, &iv[u], &qv[u]);
-                    }
+                    const int y = yb + u < wy1 ? yb + u : wy1 - 1;
+                    const int r = x - sm->off[y - ys];
+                    const int rr = r > 0 ? r : 0;
+                    const int b = static_cast<int>(fdiv_u(static_cast<unsigned int>(rr), d63));
+                    const int j = rr + b + 1;
+                    f[u] = (yb + u < wy1) && r >= 0 && j < sm->len[y - ys];
+                    const uint8_t* rec = a.raw + static_cast<long long>(y) * a.line_bytes + 2;
+                    const int id = rec[f[u] ? 64 * b : 0];
+                    const int cw = rec[f[u] ? j : 0];
+                    iv[u] = ASARF_LDG(a.lut_i + 16 * id + (cw >> 4));
+                    qv[u] = ASARF_LDG(a.lut_q + 16 * id + (cw & 15));
                 }
 #pragma unroll
                 for (int u = 0; u < kStatsBatch; ++u) {
                     const int y = yb + u;
                     if (y >= wy1) break;
-                    const double ci = iv[u], cq = qv[u];
+                    const double ci = f[u] ? iv[u] : 0.0, cq = f[u] ? qv[u] : 0.0;
                     if (y >= wy0 && f[u]) {
                         v[0] += 1.0;
                         v[1] += ci;
@@ -495,8 +499,8 @@ ASARF_HD ASARF_INLINE void raw_stats_fbaq_body(const RawStatsArgs& a, int bx, in
                             v[14] += aq * ci;
                         }
                     }
-                    pi = iv[u];
-                    pq = qv[u];
+                    pi = f[u] ? iv[u] : 0.0f;
+                    pq = f[u] ? qv[u] : 0.0f;
                     pf = f[u];
                 }
             }
@@ -539,7 +543,7 @@ ASARF_HD ASARF_INLINE void raw_stats_fbaq_body(const RawStatsArgs& a, int bx, in
 
 // Fold of the FBAQ4 partials into FloatStatAccum: over the line tiles of every
 // column tile, then over the column tiles touching each sum, both in index order.
-ASARF_HD ASARF_INLINE void stats_fold_body(const RawStatsArgs& a, int tiles_y, int tid, int nthr) {
+ASARF_HD ASARF_INLINE void stats_fold_body(const RawStatsArgs& a, int tiles_y, int tid, int nthr, double* tree) {
     const int slots = a.part_slots;
     for (int t = tid; t < a.tiles_x * slots; t += nthr) {
         double acc = a.part[t];
@@ -547,22 +551,34 @@ ASARF_HD ASARF_INLINE void stats_fold_body(const RawStatsArgs& a, int tiles_y, i
         a.part[t] = acc;
     }
     ASARF_SYNC();
-    for (int t = tid; t < 6 + 9 * a.nblk; t += nthr) {
+    // moments: pairwise tree over the column tiles (tree holds 6 x kFoldTree doubles)
+    for (int t = tid; t < 6 * kFoldTree; t += nthr) {
+        const int m = t / kFoldTree, bx = t - m * kFoldTree;
         double acc = 0.0;
-        if (t < 6) {
-            for (int bx = 0; bx < a.tiles_x; ++bx) acc += a.part[bx * slots + t];
-            a.facc->mom[t] = acc;
-        } else {
-            const int b = (t - 6) / 9, q = (t - 6) - 9 * b;
-            const int lo = (b * a.dc_step) / 32;
-            int hi = ((b + 1) * a.dc_step - 1) / 32;
-            if (hi > a.tiles_x - 1) hi = a.tiles_x - 1;
-            for (int bx = lo; bx <= hi; ++bx) {
-                const int bl = b - (bx * 32) / a.dc_step;
-                if (bl >= 0 && bl < a.span) acc += a.part[bx * slots + 6 + 9 * bl + q];
-            }
-            a.facc->lag[b][q] = acc;
+        for (int k = bx; k < a.tiles_x; k += kFoldTree) acc += a.part[k * slots + m];
+        tree[t] = acc;
+    }
+    ASARF_SYNC();
+    for (int h = kFoldTree / 2; h > 0; h >>= 1) {
+        for (int t = tid; t < 6 * h; t += nthr) {
+            const int m = t / h, i = t - m * h;
+            tree[m * kFoldTree + i] += tree[m * kFoldTree + i + h];
         }
+        ASARF_SYNC();
+    }
+    for (int t = tid; t < 6; t += nthr) a.facc->mom[t] = tree[t * kFoldTree];
+    // lag sums: the few column tiles touching each Doppler block, in order
+    for (int t = tid; t < 9 * a.nblk; t += nthr) {
+        const int b = t / 9, q = t - 9 * b;
+        const int lo = (b * a.dc_step) / 32;
+        int hi = ((b + 1) * a.dc_step - 1) / 32;
+        if (hi > a.tiles_x - 1) hi = a.tiles_x - 1;
+        double acc = 0.0;
+        for (int bx = lo; bx <= hi; ++bx) {
+            const int bl = b - (bx * 32) / a.dc_step;
+            if (bl >= 0 && bl < a.span) acc += a.part[bx * slots + 6 + 9 * bl + q];
+        }
+        a.facc->lag[b][q] = acc;
     }
 }
 

@@ -37,7 +37,8 @@ int backend_raw_stats_fbaq(const RawStatsArgs& a, int gx, int gy, void*) {
 }
 
 int backend_stats_fold(const RawStatsArgs& a, int tiles_y, void*) {
-    stats_fold_body(a, tiles_y, 0, 1);
+    std::vector<double> tree(6 * kFoldTree);
+    stats_fold_body(a, tiles_y, 0, 1, tree.data());
     return ASARF_OK;
 }
 

@@ -768,7 +768,9 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     }
     const int rc_elems = n_ctr ? ct_smem_elems_of(p->rc_len) : p->rc_len;  // compile-time lengths: padded tile
     p->raw_smem_offset = static_cast<int>((sizeof(float2) * static_cast<size_t>(rc_elems) + 127) / 128 * 128);
-    p->sh_rc = {512, static_cast<size_t>(p->raw_smem_offset) + (2 * static_cast<size_t>(s.samples_per_line) + 15) / 16 * 16};
+    const size_t raw_area = fbaq ? static_cast<size_t>(s.raw_line_bytes) + 16
+                                 : (2 * static_cast<size_t>(s.samples_per_line) + 15) / 16 * 16;
+    p->sh_rc = {512, static_cast<size_t>(p->raw_smem_offset) + raw_area};
 
     AzStridedArgs& f = p->a_fwd;
     f.in = p->bufA;

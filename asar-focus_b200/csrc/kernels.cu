@@ -24,17 +24,36 @@ __global__ void __launch_bounds__(kStatsCols, 3) k_raw_stats(RawStatsArgs a) {
     raw_stats_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, &sm);
 }
 
-__global__ void __launch_bounds__(32 * kFbaqStatsWarps) k_raw_stats_fbaq(RawStatsArgs a) {
+__global__ void __launch_bounds__(32 * kFbaqStatsWarps, 3) k_raw_stats_fbaq(RawStatsArgs a) {
     __shared__ FbaqStatsSmem sm;
     raw_stats_fbaq_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, &sm);
 }
 
 __global__ void __launch_bounds__(1024) k_stats_fold(RawStatsArgs a, int tiles_y) {
-    stats_fold_body(a, tiles_y, threadIdx.x, blockDim.x);
+    __shared__ double tree[6 * kFoldTree];
+    stats_fold_body(a, tiles_y, threadIdx.x, blockDim.x, tree);
 }
 
 __global__ void k_finalize(FinalizeArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) finalize_body(a);
+}
+
+// FBAQ4 record into shared memory: its 16-byte-aligned interior with vector loads, the
+// unaligned head and tail bytewise, so nothing outside the record is read (records are not
+// 16-byte multiples).  The copy starts at buf + (address mod 16), which keeps the interior
+// aligned in shared memory as well; buf itself is 16-byte aligned.
+__device__ __forceinline__ const uint8_t* stage_record(uint8_t* buf, const uint8_t* rec, int n) {
+    const int lead = static_cast<int>(reinterpret_cast<uintptr_t>(rec) & 15);
+    const int head = min(n, (16 - lead) & 15);
+    const int nv = (n - head) >> 4;
+    uint8_t* dst = buf + lead;
+    for (int i = threadIdx.x; i < head; i += blockDim.x) dst[i] = rec[i];
+    const uint4* src4 = reinterpret_cast<const uint4*>(rec + head);
+    uint4* dst4 = reinterpret_cast<uint4*>(dst + head);
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) dst4[i] = __ldg(src4 + i);
+    for (int i = head + 16 * nv + threadIdx.x; i < n; i += blockDim.x) dst[i] = rec[i];
+    __syncthreads();
+    return dst;
 }
 
 // One raw line per block; with bulk_bytes > 0 thread 0 fetches the line with one bulk copy
@@ -45,7 +64,10 @@ __global__ void __launch_bounds__(512) k_range_compress(RangeCompressArgs a) {
     float2* s = reinterpret_cast<float2*>(smem_rc_raw);
     __shared__ uint64_t bar;
     const uint8_t* line = nullptr;
-    if (a.bulk_bytes > 0) {
+    if constexpr (FMT == kRawAsarFbaq4) {
+        line = stage_record(smem_rc_raw + a.raw_smem_offset, a.raw + static_cast<long long>(blockIdx.x) * a.line_bytes,
+                            static_cast<int>(a.line_bytes));
+    } else if (a.bulk_bytes > 0) {
         uint8_t* buf = smem_rc_raw + a.raw_smem_offset;
         const uint8_t* src = a.raw + static_cast<long long>(blockIdx.x) * a.line_bytes;
         const int total = 2 * a.spl;
@@ -69,7 +91,10 @@ __global__ void __launch_bounds__(CtSchedule<L>::nthr, 2) k_range_compress_ct(Ra
     float2* s = reinterpret_cast<float2*>(smem_rcc_raw);
     __shared__ uint64_t bar;
     const uint8_t* line = nullptr;
-    if (a.bulk_bytes > 0) {
+    if constexpr (FMT == kRawAsarFbaq4) {
+        line = stage_record(smem_rcc_raw + a.raw_smem_offset, a.raw + static_cast<long long>(blockIdx.x) * a.line_bytes,
+                            static_cast<int>(a.line_bytes));
+    } else if (a.bulk_bytes > 0) {
         uint8_t* buf = smem_rcc_raw + a.raw_smem_offset;
         const uint8_t* src = a.raw + static_cast<long long>(blockIdx.x) * a.line_bytes;
         const int total = 2 * a.spl;
