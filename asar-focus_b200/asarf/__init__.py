@@ -42,7 +42,8 @@ class FocusPlan:
     takes host arrays and does the copies inside (the end-to-end path)."""
 
     def __init__(self, scene: Scene, rc_fft_len: int = 0, ref_compat_stats: bool = True, lib=None,
-                 lib_path=None, dc_poly=None):
+                 lib_path=None, dc_poly=None, product: int = 0, calibration: float = 1.0,
+                 record_header_bytes: int = 17, sq_stats: bool = False):
         self.lib = lib or load_library(lib_path)
         self.scene = scene
         if scene.vr_poly is None or not scene.osv:
@@ -55,6 +56,11 @@ class FocusPlan:
         if dc_poly is not None:
             opt.dc_poly_given = 1
             opt.dc_poly = (C.c_double * 3)(*[float(v) for v in dc_poly])
+        opt.product = int(product)
+        opt.calibration = float(calibration)
+        opt.record_header_bytes = int(record_header_bytes)
+        opt.sq_stats = int(bool(sq_stats))
+        self.product = int(product)
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_plan_create(C.byref(self._sc), C.byref(opt), C.byref(h)), "plan_create")
         self._h = h
@@ -68,6 +74,7 @@ class FocusPlan:
         """A view of a plan owned by someone else (a batch): never destroyed through this object."""
         self = cls.__new__(cls)
         self.lib, self.scene, self._h, self._owner = lib, scene, handle, owner
+        self.product = _lib.PRODUCT_DETECTED
         d = _lib.Dims()
         _lib.check(lib, lib.asarf_plan_dims(handle, C.byref(d)), "plan_dims")
         self.dims = {f: (list(getattr(d, f)) if f in ("out_rows", "out_cols", "vr_poly") else getattr(d, f))
@@ -89,8 +96,16 @@ class FocusPlan:
             pass
 
     @property
-    def out_shape(self) -> tuple[int, int]:
+    def out_shape(self) -> tuple:
+        """Shape of the output buffer: float32 [out_rows_max, out_cols_max] for the detected
+        image, uint8 [out_bytes_max] for level-1 MDS records."""
+        if self.product:
+            return (self.dims["out_bytes_max"],)
         return self.dims["out_rows_max"], self.dims["out_cols_max"]
+
+    @property
+    def out_dtype(self):
+        return np.uint8 if self.product else np.float32
 
     def focus(self, raw, out, swst=None, min_swst: int = 0, stream: int = 0):
         """Asynchronous focus of device-resident raw bytes into ``out`` (float32
@@ -107,10 +122,12 @@ class FocusPlan:
         if swst is not None:
             sw = np.ascontiguousarray(swst, dtype=np.uint16)
             mn = int(sw.min())
-        out = np.empty(self.out_shape, dtype=np.float32)
+        out = np.empty(self.out_shape, dtype=self.out_dtype)
         _lib.check(self.lib, self.lib.asarf_focus_host(self._h, raw.ctypes.data, _ptr(sw), mn, out.ctypes.data,
                                                        C.c_void_p(stream)), "focus_host")
         r = self.results(stream)
+        if self.product:
+            return out[: r["records"] * r["record_bytes"]].reshape(r["records"], r["record_bytes"])
         return out[: r["out_rows"], : r["out_cols"]]
 
     def focus_host_ptr(self, raw_ptr: int, out_ptr: int, swst_ptr: int = 0, min_swst: int = 0, stream: int = 0):

@@ -36,7 +36,13 @@ RAW_ASAR_FBAQ4 = 1
 
 class Options(C.Structure):
     _fields_ = [("rc_fft_len", C.c_int32), ("ref_compat_stats", C.c_int32), ("iq_padding_ref", C.c_int32),
-                ("dc_poly_given", C.c_int32), ("dc_poly", C.c_double * 3)]
+                ("dc_poly_given", C.c_int32), ("dc_poly", C.c_double * 3), ("product", C.c_int32),
+                ("record_header_bytes", C.c_int32), ("calibration", C.c_float), ("sq_stats", C.c_int32)]
+
+
+PRODUCT_DETECTED = 0
+PRODUCT_IMP_MDS = 1
+PRODUCT_IMS_MDS = 2
 
 
 class Dims(C.Structure):
@@ -45,6 +51,7 @@ class Dims(C.Structure):
         ("n1", C.c_int32), ("n2", C.c_int32), ("slc_cols", C.c_int32), ("out_rows", C.c_int32 * 2),
         ("out_cols", C.c_int32 * 2), ("out_rows_max", C.c_int32), ("out_cols_max", C.c_int32),
         ("max_aperture", C.c_int32), ("vr_poly", C.c_double * 3), ("device_bytes", C.c_size_t),
+        ("out_bytes_max", C.c_int64),
     ]
 
 
@@ -55,7 +62,8 @@ class Results(C.Structure):
         ("doppler_centroid_estimate", C.c_double * 3),
         ("vr_poly", C.c_double * 3), ("n_dc_blocks", C.c_int32), ("dc_block_hz", C.c_double * 80),
         ("variant", C.c_int32), ("first_line", C.c_int32), ("n_lines", C.c_int32), ("out_rows", C.c_int32),
-        ("out_cols", C.c_int32), ("errors", C.c_uint32),
+        ("out_cols", C.c_int32), ("errors", C.c_uint32), ("records", C.c_int32), ("record_bytes", C.c_int32),
+        ("sq_stats", C.c_double * 4),
     ]
 
 
@@ -103,6 +111,10 @@ _SIGS = {
     "asarf_convert_asar_blocks": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
     "asarf_fbaq4_index": (C.c_int32, [C.c_int32, C.c_int32]),
+    "asarf_condition_slc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_void_p,
+                                      C.c_void_p]),
+    "asarf_condition_detected": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_void_p,
+                                           C.c_void_p]),
     "asarf_focus_host_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "asarf_plan_wait": (C.c_int, [C.c_void_p]),
     "asarf_plan_slc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

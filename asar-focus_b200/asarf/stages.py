@@ -91,6 +91,28 @@ def convert_asar_blocks(raw, img, range_size: int, lut_i, lut_q, swst=None, min_
     _lib.check(lib, rc, "convert_asar_blocks")
 
 
+def condition_slc(img, x_size: int, dest, record_header_bytes: int = 17, calibration: float = 1.0,
+                  lib=None) -> None:
+    """ConditionResultsSLC (envisat_format/src/envisat_format_kernels.cu:28-61, 95-106): complex
+    ``img`` [rows][stride] (first x_size columns) -> IMS MDS records in ``dest``
+    (rows x (header + 4 x_size) bytes)."""
+    lib = lib or load_library()
+    rows, stride = int(img.shape[0]), int(img.shape[1])
+    rc = lib.asarf_condition_slc(_ptr(img), int(x_size), rows, stride, int(record_header_bytes), float(calibration),
+                                 _ptr(dest), _stream(img))
+    _lib.check(lib, rc, "condition_slc")
+
+
+def condition_detected(img, dest, record_header_bytes: int = 17, calibration: float = 1.0, lib=None) -> None:
+    """ConditionResultsDetected (envisat_format/src/envisat_format_kernels.cu:63-93, 108-114): float
+    ``img`` [rows][cols] -> IMP MDS records in ``dest`` (rows x (header + 2 cols) bytes)."""
+    lib = lib or load_library()
+    rows, cols = int(img.shape[0]), int(img.shape[1])
+    rc = lib.asarf_condition_detected(_ptr(img), cols, rows, int(record_header_bytes), float(calibration), _ptr(dest),
+                                      _stream(img))
+    _lib.check(lib, rc, "condition_detected")
+
+
 def raw_data_correction(img: DevicePaddedImage, n_total_samples: int, lib=None) -> dict:
     """RawDataCorrection (sar/iq_correction.cu:188-274) in place; returns the SARResults
     fields it sets."""

@@ -25,6 +25,8 @@ int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int 
 int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, unsigned int* err,
                   void* stream);
 int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err, void* stream);
+int backend_condition(const ConditionArgs& a, int rows, void* stream);
+int backend_product_stats(const ProductStatsArgs& a, void* stream);  // partials then fold
 
 // per-stage kernels
 int backend_decode(const DecodeArgs& a, long long n, void* stream);

@@ -1029,6 +1029,70 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     }
 }
 
+// ----------------------------------------------------------------------------- L1 product records
+// Envisat MDS records of the level-1 products (ConditionResultsSLC / ConditionResultsDetected,
+// envisat_format/src/envisat_format_kernels.cu:28-114): `hdr` zero bytes of record header, then
+// the pixels.  IMS: I and Q of a complex pixel times the calibration constant, clamped to the
+// int16 range and truncated toward zero (NaN gives 0), big-endian.  IMP: 10 log10 of the
+// intensity times the constant, capped at 65535 and truncated to uint16 (negative, -inf and NaN
+// give 0), least significant byte first as the reference kernel stores it.
+ASARF_HD ASARF_INLINE int f2i_rz(float v) {
+#if defined(__CUDA_ARCH__)
+    return __float2int_rz(v);  // NaN -> 0
+#else
+    return v != v ? 0 : static_cast<int>(v);
+#endif
+}
+
+ASARF_HD ASARF_INLINE unsigned int f2u_rz(float v) {
+#if defined(__CUDA_ARCH__)
+    return __float2uint_rz(v);  // negative, NaN -> 0
+#else
+    return (v != v || v <= 0.0f) ? 0u : static_cast<unsigned int>(v);
+#endif
+}
+
+ASARF_HD ASARF_INLINE float log10_f32(float x) {
+#if defined(__CUDA_ARCH__)
+    return log10f(x);
+#else
+    return static_cast<float>(__builtin_log10(static_cast<double>(x)));
+#endif
+}
+
+ASARF_HD ASARF_INLINE int ims_value(float v, float cal) {
+    const float s = fmul_rn(v, cal);
+    const float c = s > 32767.0f ? 32767.0f : (s < -32768.0f ? -32768.0f : s);
+    return f2i_rz(c);
+}
+
+ASARF_HD ASARF_INLINE unsigned int imp_value(float v, float cal) {
+    const float db = fmul_rn(10.0f, log10_f32(fmul_rn(v, cal)));
+    return f2u_rz(65535.0f < db ? 65535.0f : db);
+}
+
+// One IMS record: row of x_size complex pixels -> dest (header + 4 bytes per pixel).
+ASARF_HD ASARF_INLINE void ims_record(const float2* row, int x_size, float cal, int hdr, uint8_t* dest, int tid,
+                                      int nthr) {
+    for (int i = tid; i < hdr; i += nthr) dest[i] = 0;
+    uint8_t* d = dest + hdr;
+    for (int x = tid; x < x_size; x += nthr) {
+        const float2 v = row[x];
+        const int i = ims_value(v.x, cal), q = ims_value(v.y, cal);
+        d[4 * x + 0] = static_cast<uint8_t>((i >> 8) & 0xff);
+        d[4 * x + 1] = static_cast<uint8_t>(i & 0xff);
+        d[4 * x + 2] = static_cast<uint8_t>((q >> 8) & 0xff);
+        d[4 * x + 3] = static_cast<uint8_t>(q & 0xff);
+    }
+}
+
+// IMP pixel x of a record payload.
+ASARF_HD ASARF_INLINE void imp_store(uint8_t* payload, int x, float v, float cal) {
+    const unsigned int u = imp_value(v, cal);
+    payload[2 * x] = static_cast<uint8_t>(u & 0xff);
+    payload[2 * x + 1] = static_cast<uint8_t>((u >> 8) & 0xff);
+}
+
 // ----------------------------------------------------------------------------- detected tail
 // One output line per block: results-window subset (main_flow.cc:585-627), time-domain
 // azimuth multilook (TimeDomainAzimuthLook, sar/az_multilook.cu:25-80), range spreading loss
@@ -1070,7 +1134,10 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
         ml[c] = fmul_rn(val, ASARF_LDG(tv.rsl + c));
     }
     ASARF_SYNC();
-    float* orow = a.out + static_cast<long long>(y) * a.out_pitch;
+    float* orow = a.mds ? nullptr : a.out + static_cast<long long>(y) * a.out_pitch;
+    uint8_t* rec = a.mds ? a.mds + static_cast<long long>(y) * (a.mds_hdr + 2 * tv.ng) : nullptr;
+    if (rec)
+        for (int i = tid; i < a.mds_hdr; i += nthr) rec[i] = 0;
     for (int xg = tid; xg < tv.ng; xg += nthr) {
         const float gd = fmul_rn(static_cast<float>(xg), a.ground_spacing);
         const float rd = polyval_f32(tv.grsr, gd);
@@ -1082,7 +1149,138 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
             i0 = i0 < 0 ? 0 : a.nx - 2;
         }
         const float v0 = ml[i0], v1 = ml[i0 + 1];
-        orow[xg] = fma_rn(dx, fsub_rn(v1, v0), v0);
+        const float v = fma_rn(dx, fsub_rn(v1, v0), v0);
+        if (rec)
+            imp_store(rec + a.mds_hdr, xg, v, a.mds_cal);
+        else
+            orow[xg] = v;
+        if (a.out2) a.out2[static_cast<long long>(y) * a.out_pitch + xg] = v;
+    }
+}
+
+// One record of a level-1 product (row y of the input).
+ASARF_HD ASARF_INLINE void condition_row(const ConditionArgs& a, int y, int tid, int nthr) {
+    if (a.product == 2) {
+        const float2* base = a.slc;
+        int rows = a.y_size;
+        if (a.state) {
+            base += static_cast<long long>(a.state->first_line) * a.stride;
+            rows = a.state->n_lines;
+        }
+        if (y >= rows) return;
+        ims_record(base + static_cast<long long>(y) * a.stride, a.x_size, a.cal, a.hdr,
+                   a.dest + static_cast<long long>(y) * (a.hdr + 4ll * a.x_size), tid, nthr);
+    } else {
+        if (y >= a.y_size) return;
+        uint8_t* rec = a.dest + static_cast<long long>(y) * (a.hdr + 2ll * a.x_size);
+        for (int i = tid; i < a.hdr; i += nthr) rec[i] = 0;
+        const float* row = a.img + static_cast<long long>(y) * a.stride;
+        for (int x = tid; x < a.x_size; x += nthr) imp_store(rec + a.hdr, x, row[x], a.cal);
+    }
+}
+
+// ----------------------------------------------------------------------------- product statistics
+// Pair p of the product statistics.  IMS form: SLC pixel p of the results window.  IMP form: the
+// reference reuses the subset SLC's buffer for the ground-range floats and views it as a
+// complex image of the ground-range size (main.cc:327-331), so pair p is floats 2p, 2p+1 of
+// that buffer: ground-range pixels below N = ng * out_az, beyond it the SLC floats the
+// resampling did not overwrite (SLC stored contiguously [lines][nx], as the subset copy leaves it).
+ASARF_HD ASARF_INLINE float stats_float(const ProductStatsArgs& a, long long f, long long n_img, int ng) {
+    if (f < n_img) {
+        const long long r = f / ng;
+        return a.img[r * a.img_pitch + (f - r * ng)];
+    }
+    const long long k = f >> 1;
+    const long long r = k / a.nx;
+    const float2 z = a.slc[(a.state->first_line + r) * a.slc_pitch + (k - r * a.nx)];
+    return (f & 1) ? z.y : z.x;
+}
+
+ASARF_HD ASARF_INLINE long long stats_pairs(const ProductStatsArgs& a) {
+    const FocusState& st = *a.state;
+    return a.imaged ? static_cast<long long>(a.ng[st.variant]) * a.out_az[st.variant]
+                    : static_cast<long long>(st.n_lines) * a.nx;
+}
+
+// Block `blk` of `a.blocks`: pairs blk * 256 + t, stepping by blocks * 256, into part[blk]
+// (pairwise tree over the 256 lanes).
+ASARF_HD ASARF_INLINE void product_stats_body(const ProductStatsArgs& a, int blk, int tid, int nthr, double* red) {
+    const FocusState& st = *a.state;
+    const long long n = stats_pairs(a);
+    const int ng = a.ng[st.variant];
+    const long long n_img = static_cast<long long>(ng) * a.out_az[st.variant];
+    for (int t = tid; t < 256; t += nthr) {
+        double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (long long p = static_cast<long long>(blk) * 256 + t; p < n; p += static_cast<long long>(a.blocks) * 256) {
+            float x, y;
+            if (a.imaged) {
+                x = stats_float(a, 2 * p, n_img, ng);
+                y = stats_float(a, 2 * p + 1, n_img, ng);
+            } else {
+                const long long r = p / a.nx;
+                const float2 z = a.slc[(st.first_line + r) * a.slc_pitch + (p - r * a.nx)];
+                x = z.x;
+                y = z.y;
+            }
+            if (x != x || y != y) continue;
+            v[0] += 1.0;
+            v[1] += x;
+            v[2] += y;
+            v[3] += static_cast<double>(x) * x;
+            v[4] += static_cast<double>(y) * y;
+        }
+        for (int k = 0; k < 5; ++k) red[k * 256 + t] = v[k];
+    }
+    ASARF_SYNC();
+    for (int h = 128; h > 0; h >>= 1) {
+        for (int t = tid; t < 5 * h; t += nthr) {
+            const int k = t / h, i = t - k * h;
+            red[k * 256 + i] += red[k * 256 + i + h];
+        }
+        ASARF_SYNC();
+    }
+    for (int k = tid; k < 5; k += nthr) a.part[static_cast<long long>(blk) * 5 + k] = red[k * 256];
+}
+
+// Fold of the block partials (pairwise tree over kStatsFoldLeaves leaves) and the statistics in
+// the reference's arithmetic: mean = float(float(sum) / float(N)), deviation = sqrt(float(
+// float(sum of squared differences) / float(N))) with N all pairs, as CalcMean / CalcStdDev
+// divide by the image size; IMS: (mean I, mean Q, dev I, dev Q), IMP: ((mean I + mean Q) / 2, 0,
+// (dev I + dev Q) / 2, 0); then scaled by the calibration constant as main.cc:336-342, 384-390.
+constexpr int kStatsFoldLeaves = 1024;
+ASARF_HD ASARF_INLINE void product_stats_fold(const ProductStatsArgs& a, int tid, int nthr, double* tree) {
+    for (int t = tid; t < 5 * kStatsFoldLeaves; t += nthr) {
+        const int k = t / kStatsFoldLeaves, i = t - k * kStatsFoldLeaves;
+        tree[t] = i < a.blocks ? a.part[static_cast<long long>(i) * 5 + k] : 0.0;
+    }
+    ASARF_SYNC();
+    for (int h = kStatsFoldLeaves / 2; h > 0; h >>= 1) {
+        for (int t = tid; t < 5 * h; t += nthr) {
+            const int k = t / h, i = t - k * h;
+            tree[k * kStatsFoldLeaves + i] += tree[k * kStatsFoldLeaves + i + h];
+        }
+        ASARF_SYNC();
+    }
+    if (tid != 0) return;
+    const double cnt = tree[0], sx = tree[kStatsFoldLeaves], sy = tree[2 * kStatsFoldLeaves];
+    const double sxx = tree[3 * kStatsFoldLeaves], syy = tree[4 * kStatsFoldLeaves];
+    const float nf = static_cast<float>(stats_pairs(a));
+    const float mx = static_cast<float>(sx) / nf, my = static_cast<float>(sy) / nf;
+    const double dx = sxx - 2.0 * mx * sx + cnt * static_cast<double>(mx) * mx;
+    const double dy = syy - 2.0 * my * sy + cnt * static_cast<double>(my) * my;
+    const float vx = static_cast<float>(dx) / nf, vy = static_cast<float>(dy) / nf;
+    const float ex = sqrtf(vx), ey = sqrtf(vy);
+    const double c = a.cal;
+    if (a.imaged) {
+        a.out[0] = static_cast<double>((mx + my) / 2) * c;
+        a.out[1] = 0.0;
+        a.out[2] = static_cast<double>((ex + ey) / 2) * c;
+        a.out[3] = 0.0;
+    } else {
+        a.out[0] = mx * c;
+        a.out[1] = my * c;
+        a.out[2] = ex * c;
+        a.out[3] = ey * c;
     }
 }
 

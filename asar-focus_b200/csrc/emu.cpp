@@ -111,6 +111,18 @@ int backend_decode(const DecodeArgs& a, long long n, void*) {
     for (long long i = 0; i < n; ++i) decode_item(a, i);
     return ASARF_OK;
 }
+int backend_product_stats(const ProductStatsArgs& a, void*) {
+    std::vector<double> red(5 * 256), tree(5 * kStatsFoldLeaves);
+    for (int b = 0; b < a.blocks; ++b) product_stats_body(a, b, 0, 1, red.data());
+    product_stats_fold(a, 0, 1, tree.data());
+    return ASARF_OK;
+}
+
+int backend_condition(const ConditionArgs& a, int rows, void*) {
+    for (int y = 0; y < rows; ++y) condition_row(a, y, 0, 1);
+    return ASARF_OK;
+}
+
 int backend_decode_fbaq(const DecodeFbaqArgs& a, long long n, void*) {
     for (long long i = 0; i < n; ++i) decode_fbaq_item(a, i);
     return ASARF_OK;

@@ -386,6 +386,10 @@ void asarf_default_options(asarf_options* opt) {
     opt->iq_padding_ref = 0;
     opt->dc_poly_given = 0;
     opt->dc_poly[0] = opt->dc_poly[1] = opt->dc_poly[2] = 0.0;
+    opt->product = ASARF_PRODUCT_DETECTED;
+    opt->record_header_bytes = 17;  // main.cc: 12 + 1 + 4
+    opt->calibration = 1.0f;
+    opt->sq_stats = 0;
 }
 
 int32_t asarf_fft_size_above(int32_t v) { return fft_size_above(v); }
@@ -616,6 +620,20 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     }
     p->out_rows_max = std::max(out_az[0], out_az[1]);
     p->out_cols_max = std::max(ng[0], ng[1]);
+    if (opt.product < ASARF_PRODUCT_DETECTED || opt.product > ASARF_PRODUCT_IMS_MDS || opt.record_header_bytes < 0) {
+        delete p;
+        return set_error(ASARF_ERR_INVALID, "unknown product %d or negative record header", opt.product);
+    }
+    {
+        const long long hdr = opt.record_header_bytes;
+        long long bytes = 4ll * p->out_rows_max * p->out_cols_max;
+        for (int v = 0; v < 2; ++v) {
+            if (opt.product == ASARF_PRODUCT_IMP_MDS) bytes = std::max(bytes, out_az[v] * (hdr + 2ll * ng[v]));
+            if (opt.product == ASARF_PRODUCT_IMS_MDS) bytes = std::max(bytes, n_lines[v] * (hdr + 4ll * p->nx));
+        }
+        p->out_bytes = bytes;
+        p->ims_rows_max = std::max(n_lines[0], n_lines[1]);
+    }
     std::vector<float> rsl(p->nx);
     for (int i = 0; i < p->nx; ++i) {
         const double R = sub_first + i * s.range_spacing;
@@ -631,7 +649,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     p->state = p->alloc<FocusState>(1);
     p->raw_dev = p->alloc<uint8_t>(static_cast<size_t>(p->na) * s.raw_line_bytes);
     p->swst_dev = p->alloc<uint16_t>(p->na);
-    p->out_dev = p->alloc<float>(static_cast<size_t>(p->out_rows_max) * p->out_cols_max);
+    p->out_dev = p->alloc<float>(static_cast<size_t>(p->out_bytes + 3) / 4);
     float2* rc_tw = p->alloc<float2>(p->rc_len);
     p->rc_mf = p->alloc<float2>(p->rc_len);
     float2* ct_tw = ctw.empty() ? nullptr : p->alloc<float2>(ctw.size());
@@ -657,8 +675,11 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     float* lut_dev = fbaq ? p->alloc<float>(2 * 4096) : nullptr;
     double* part_dev = fbaq ? p->alloc<double>(static_cast<size_t>(fb_tiles_y) * fb_tiles_x * fb_slots) : nullptr;
     FloatStatAccum* facc_dev = fbaq ? p->alloc<FloatStatAccum>(1) : nullptr;
+    constexpr int kPstatBlocks = 4 * 148;
+    double* pstat_dev = opt.sq_stats ? p->alloc<double>(5 * kPstatBlocks + 4) : nullptr;
     if (!p->bufA || !p->bufB || !p->acc || !p->state || !p->raw_dev || !p->swst_dev || !p->out_dev || !rc_tw ||
-        !p->rc_mf || !tw1 || !drev1 || !tw2 || !drev2 || !twN || !win || !rsl_dev || (fbaq && (!lut_dev || !part_dev || !facc_dev))) {
+        !p->rc_mf || !tw1 || !drev1 || !tw2 || !drev2 || !twN || !win || !rsl_dev || (fbaq && (!lut_dev || !part_dev || !facc_dev)) ||
+        (opt.sq_stats && !pstat_dev)) {
         const size_t need = p->bytes;
         delete p;
         return set_error(ASARF_ERR_NOMEM, "device allocation failed (plan needs about %zu MB)",
@@ -842,7 +863,26 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     t.range_spacing = static_cast<float>(s.range_spacing);
     t.ground_spacing = kGroundSpacing;
     t.out_pitch = p->out_cols_max;
+    t.mds_hdr = opt.record_header_bytes;
+    t.mds_cal = opt.calibration;
     p->sh_tail = {256, sizeof(float) * static_cast<size_t>(p->nx)};
+    if (opt.sq_stats) {
+        ProductStatsArgs& ps = p->a_pstats;
+        ps.imaged = opt.product == ASARF_PRODUCT_IMS_MDS ? 0 : 1;
+        ps.slc = p->bufB + kRcmcTaps / 2;
+        ps.slc_pitch = p->pitch;
+        ps.nx = p->nx;
+        ps.img_pitch = p->out_cols_max;
+        for (int v = 0; v < 2; ++v) {
+            ps.ng[v] = ng[v];
+            ps.out_az[v] = out_az[v];
+        }
+        ps.state = p->state;
+        ps.part = pstat_dev;
+        ps.blocks = kPstatBlocks;
+        ps.cal = opt.calibration;
+        ps.out = pstat_dev + 5 * kPstatBlocks;
+    }
 
     // ---- TMA tensor maps (all tiles come from this GPU's own buffers; loads only)
     {
@@ -892,6 +932,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     }
     dm.out_rows_max = p->out_rows_max;
     dm.out_cols_max = p->out_cols_max;
+    dm.out_bytes_max = p->out_bytes;
     dm.max_aperture = max_ap;
     for (int k = 0; k < 3; ++k) dm.vr_poly[k] = p->vr_poly[k];
     dm.device_bytes = p->bytes;
@@ -966,10 +1007,34 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     rc = backend_az_strided(p->a_inv, p->use_tma ? p->tmapB3 : nullptr, p->tiles1, p->n2, p->sh_st, stream);
     if (rc) return rc;
     mark();
-    if (!p->skip_tail) {
+    if (!p->skip_tail && p->opt.product == ASARF_PRODUCT_IMS_MDS) {
+        ConditionArgs c{};
+        c.product = 2;
+        c.slc = p->bufB + kRcmcTaps / 2;
+        c.stride = p->pitch;
+        c.x_size = p->nx;
+        c.hdr = p->opt.record_header_bytes;
+        c.cal = p->opt.calibration;
+        c.dest = reinterpret_cast<uint8_t*>(d_out);
+        c.state = p->state;
+        rc = backend_condition(c, p->ims_rows_max, stream);
+        if (rc) return rc;
+    } else if (!p->skip_tail) {
         TailArgs t = p->a_tail;
         t.out = d_out;
+        if (p->opt.product == ASARF_PRODUCT_IMP_MDS) {
+            t.mds = reinterpret_cast<uint8_t*>(d_out);
+            // the statistics read the float image, which the records do not keep: bufA is
+            // free once the inverse azimuth pass has run
+            if (p->opt.sq_stats) t.out2 = reinterpret_cast<float*>(p->bufA);
+        }
         rc = backend_tail(t, p->out_rows_max, p->sh_tail, &p->state->errors, stream);
+        if (rc) return rc;
+    }
+    if (!p->skip_tail && p->opt.sq_stats) {
+        ProductStatsArgs ps = p->a_pstats;
+        ps.img = p->opt.product == ASARF_PRODUCT_DETECTED ? d_out : reinterpret_cast<float*>(p->bufA);
+        rc = backend_product_stats(ps, stream);
         if (rc) return rc;
     }
     mark();
@@ -1024,8 +1089,7 @@ static int enqueue_host_run(asarf_plan* p, const uint8_t* h_raw, const uint16_t*
     }
     rc = asarf_focus(p, p->raw_dev, h_swst ? p->swst_dev : nullptr, min_swst, p->out_dev, stream);
     if (rc) return rc;
-    return mem_d2h(h_out, p->out_dev, sizeof(float) * static_cast<size_t>(p->out_rows_max) * p->out_cols_max,
-                   stream);
+    return mem_d2h(h_out, p->out_dev, static_cast<size_t>(p->out_bytes), stream);
 }
 
 extern "C" {
@@ -1085,6 +1149,22 @@ int asarf_plan_results(asarf_plan* p, asarf_results* res, void* stream) {
     res->out_rows = p->dims.out_rows[st.variant & 1];
     res->out_cols = p->dims.out_cols[st.variant & 1];
     res->errors = st.errors;
+    if (p->opt.sq_stats) {
+        rc = mem_d2h(res->sq_stats, p->a_pstats.out, sizeof(res->sq_stats), stream);
+        if (!rc) rc = stream_sync(stream);
+        if (rc) return rc;
+    }
+    const int hdr = p->opt.record_header_bytes;
+    if (p->opt.product == ASARF_PRODUCT_IMP_MDS) {
+        res->records = res->out_rows;
+        res->record_bytes = hdr + 2 * res->out_cols;
+    } else if (p->opt.product == ASARF_PRODUCT_IMS_MDS) {
+        res->records = st.n_lines;
+        res->record_bytes = hdr + 4 * p->nx;
+    } else {
+        res->records = res->out_rows;
+        res->record_bytes = 4 * p->out_cols_max;
+    }
     return ASARF_OK;
 }
 

@@ -34,6 +34,20 @@ __global__ void __launch_bounds__(1024) k_stats_fold(RawStatsArgs a, int tiles_y
     stats_fold_body(a, tiles_y, threadIdx.x, blockDim.x, tree);
 }
 
+__global__ void __launch_bounds__(256) k_product_stats(ProductStatsArgs a) {
+    __shared__ double red[5 * 256];
+    product_stats_body(a, blockIdx.x, threadIdx.x, blockDim.x, red);
+}
+
+__global__ void __launch_bounds__(1024) k_product_stats_fold(ProductStatsArgs a) {
+    __shared__ double tree[5 * kStatsFoldLeaves];
+    product_stats_fold(a, threadIdx.x, blockDim.x, tree);
+}
+
+__global__ void __launch_bounds__(256) k_condition(ConditionArgs a) {
+    condition_row(a, blockIdx.x, threadIdx.x, blockDim.x);
+}
+
 __global__ void k_finalize(FinalizeArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) finalize_body(a);
 }
@@ -337,6 +351,18 @@ int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err,
 int backend_decode(const DecodeArgs& a, long long n, void* stream) {
     k_items<DecodeArgs, decode_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);
     return check_launch("decode");
+}
+int backend_product_stats(const ProductStatsArgs& a, void* stream) {
+    k_product_stats<<<a.blocks, 256, 0, S(stream)>>>(a);
+    int rc = check_launch("product_stats");
+    if (rc) return rc;
+    k_product_stats_fold<<<1, 1024, 0, S(stream)>>>(a);
+    return check_launch("product_stats_fold");
+}
+int backend_condition(const ConditionArgs& a, int rows, void* stream) {
+    if (rows <= 0) return ASARF_OK;
+    k_condition<<<rows, 256, 0, S(stream)>>>(a);
+    return check_launch("condition");
 }
 int backend_decode_fbaq(const DecodeFbaqArgs& a, long long n, void* stream) {
     k_items<DecodeFbaqArgs, decode_fbaq_item><<<grid_for(n), 256, 0, S(stream)>>>(a, n);

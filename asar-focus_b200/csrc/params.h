@@ -194,6 +194,44 @@ struct TailArgs {
     float ground_spacing;
     float* out;
     int out_pitch;
+    // IMP product records instead of the float image (mds != nullptr): record y at
+    // mds + y * (mds_hdr + 2 * ng), ng of the chosen variant; with out2 the float image is
+    // also stored there (pitch out_pitch) for the product statistics
+    float* out2;
+    uint8_t* mds;
+    int mds_hdr;
+    float mds_cal;
+};
+
+// Statistics of the level-1 product written into its SQ ADS (CalculateStatistics /
+// CalculateStatisticsImaged, main_flow.cc:666-676, through DevicePaddedImage::CalcMean /
+// CalcStdDev): FP64 sums over pairs (x, y), pairs holding a NaN skipped.
+struct ProductStatsArgs {
+    int imaged;             // 1: IMP form, 0: IMS form (pairs = complex SLC pixels)
+    const float2* slc;      // SLC of the results window starts at row state->first_line
+    long long slc_pitch;
+    int nx;                 // SLC columns
+    const float* img;       // IMP form: ground-range float image [out_az][img_pitch]
+    int img_pitch;
+    int ng[kNumTailVariants], out_az[kNumTailVariants];
+    const FocusState* state;
+    double* part;           // [blocks][5]: pairs counted, sum x, sum y, sum x^2, sum y^2
+    int blocks;
+    float cal;
+    double* out;            // 4 statistics as main.cc hands them to the product header
+};
+
+// Level-1 product records (ConditionResultsSLC / ConditionResultsDetected).
+struct ConditionArgs {
+    int product;            // 1: IMP from img, 2: IMS from slc
+    const float* img;       // IMP input [y][stride]
+    const float2* slc;      // IMS input [y][stride]
+    long long stride;       // elements per input row
+    int x_size, y_size;
+    int hdr;                // record header bytes (zeroed)
+    float cal;              // calibration constant
+    uint8_t* dest;
+    const FocusState* state;  // fused IMS: rows first_line .. first_line + n_lines of slc
 };
 
 // ------------------------------------------------------------------ per-stage entry points

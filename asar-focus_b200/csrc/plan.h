@@ -20,6 +20,7 @@ using asarf::RangeCompressArgs;
 using asarf::RawStatsArgs;
 using asarf::StatAccum;
 using asarf::TailArgs;
+using asarf::ProductStatsArgs;
 using asarf::event_destroy;
 using asarf::mem_alloc;
 using asarf::mem_free;
@@ -59,6 +60,9 @@ struct asarf_plan {
     LaunchShape sh_rc{}, sh_st{}, sh_rd{}, sh_tail{};
     int tiles1 = 0, tiles2 = 0;
     int out_rows_max = 0, out_cols_max = 0;
+    long long out_bytes = 0;      // bytes written at d_out for the product
+    int ims_rows_max = 0;         // IMS records: most lines a results window keeps
+    ProductStatsArgs a_pstats{};  // SQ ADS statistics (opt.sq_stats)
     // optional per-kernel timing (events recorded between the launches of each run)
     std::vector<void*> events;
     int timing_slots = 0, timing_used = 0;

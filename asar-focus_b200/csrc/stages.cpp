@@ -112,6 +112,42 @@ int asarf_convert_asar_blocks(const uint8_t* d_raw, int32_t record_bytes, int32_
 
 int32_t asarf_fbaq4_index(int32_t block, int32_t code) { return fbaq4_index(block, code); }
 
+int asarf_condition_slc(const void* d_img, int32_t x_size, int32_t y_size, int32_t x_stride,
+                        int32_t record_header_bytes, float calibration, void* d_dest, void* stream) {
+    if (!d_img || !d_dest || x_size <= 0 || y_size <= 0 || x_stride < x_size || record_header_bytes < 0)
+        return set_error(ASARF_ERR_INVALID, "condition_slc: bad arguments");
+    ConditionArgs c{};
+    c.product = 2;
+    c.slc = static_cast<const float2*>(d_img);
+    c.stride = x_stride;
+    c.x_size = x_size;
+    c.y_size = y_size;
+    c.hdr = record_header_bytes;
+    c.cal = calibration;
+    c.dest = static_cast<uint8_t*>(d_dest);
+    int rc = backend_condition(c, y_size, stream);
+    if (rc) return rc;
+    return stream_sync(stream);
+}
+
+int asarf_condition_detected(const float* d_img, int32_t range_size, int32_t azimuth_size,
+                             int32_t record_header_bytes, float calibration, void* d_dest, void* stream) {
+    if (!d_img || !d_dest || range_size <= 0 || azimuth_size <= 0 || record_header_bytes < 0)
+        return set_error(ASARF_ERR_INVALID, "condition_detected: bad arguments");
+    ConditionArgs c{};
+    c.product = 1;
+    c.img = d_img;
+    c.stride = range_size;
+    c.x_size = range_size;
+    c.y_size = azimuth_size;
+    c.hdr = record_header_bytes;
+    c.cal = calibration;
+    c.dest = static_cast<uint8_t*>(d_dest);
+    int rc = backend_condition(c, azimuth_size, stream);
+    if (rc) return rc;
+    return stream_sync(stream);
+}
+
 int asarf_raw_data_correction(void* d_img, int32_t x_size, int32_t y_size, int32_t x_stride, int32_t y_stride,
                               int64_t n_total_samples, asarf_iq_results* results, void* stream) {
     if (!d_img || !results || x_size <= 0 || y_size <= 0 || x_stride < x_size || y_stride < y_size)

@@ -80,6 +80,13 @@ typedef struct asarf_scene {
     const float* fbaq_q_lut;
 } asarf_scene;
 
+/* What asarf_focus writes at d_out (asarf_options.product). */
+#define ASARF_PRODUCT_DETECTED 0  /* float ground-range intensity [out_rows][out_cols_max] */
+#define ASARF_PRODUCT_IMP_MDS 1   /* IMP level-1 MDS records: out_rows records of header + 2*out_cols bytes
+                                     (FormatResultsDetected, main.cc:345-370) */
+#define ASARF_PRODUCT_IMS_MDS 2   /* IMS level-1 MDS records of the complex SLC: n_lines records of
+                                     header + 4*slc_cols bytes (FormatResultsSLC, main.cc:378-420) */
+
 /* Options of the fused plan. */
 typedef struct asarf_options {
     int32_t rc_fft_len;        /* range FFT length; 0 = auto (any >= range_size gives the same result) */
@@ -87,6 +94,11 @@ typedef struct asarf_options {
     int32_t iq_padding_ref;    /* range padding the reference would use for those sums; 0 = its own rule */
     int32_t dc_poly_given;     /* 1: use dc_poly instead of the ACCC estimate (the estimate is still reported) */
     double dc_poly[3];         /* Doppler centroid polynomial (range pixel), highest power first */
+    int32_t product;           /* ASARF_PRODUCT_* (default ASARF_PRODUCT_DETECTED) */
+    int32_t record_header_bytes; /* MDS record header, zero-filled (main.cc: 12 + 1 + 4 = 17, the default) */
+    float calibration;         /* MDS calibration constant (main.cc: process gain / sqrt(scaling factor));
+                                  default 1 */
+    int32_t sq_stats;          /* 1: also compute the product statistics of the SQ ADS (asarf_results.sq_stats) */
 } asarf_options;
 
 /* Output geometry of a plan (both tail variants: the Doppler-centroid sign picks one). */
@@ -101,6 +113,7 @@ typedef struct asarf_dims {
     int32_t max_aperture;
     double vr_poly[3];
     size_t device_bytes;       /* device memory held by the plan */
+    int64_t out_bytes_max;     /* bytes asarf_focus may write at d_out for the plan's product */
 } asarf_dims;
 
 /* Per-run results: SARResults (sar/sar_metadata.h:46-55) plus the chosen window. */
@@ -113,6 +126,13 @@ typedef struct asarf_results {
     double dc_block_hz[80];
     int32_t variant, first_line, n_lines, out_rows, out_cols;
     uint32_t errors;
+    int32_t records, record_bytes;  /* rows written at d_out and their byte stride (product layout) */
+    /* with asarf_options.sq_stats: the statistics main.cc writes into the product header,
+     * scaled by the calibration constant as there (main.cc:331-342 IMP, 380-390 IMS):
+     * IMS (mean I, mean Q, std I, std Q) of the SLC (CalculateStatistics, main_flow.cc:666-670);
+     * otherwise the IMP form ((mean I + mean Q) / 2, 0, (std I + std Q) / 2, 0) over the
+     * ground-range buffer viewed as complex (CalculateStatisticsImaged, main_flow.cc:672-676) */
+    double sq_stats[4];
 } asarf_results;
 
 typedef struct asarf_plan asarf_plan;
@@ -129,8 +149,9 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt, asarf_
 void asarf_plan_destroy(asarf_plan* plan);
 int asarf_plan_dims(const asarf_plan* plan, asarf_dims* dims);
 
-/* Focus one scene from device-resident raw bytes to the detected ground-range image
- * (float [out_rows][out_cols_max], row pitch out_cols_max).  Replaces main.cc:233-327:
+/* Focus one scene from device-resident raw bytes to the plan's product at d_out (default: the
+ * detected ground-range image, float [out_rows][out_cols_max], row pitch out_cols_max; see
+ * ASARF_PRODUCT_* for the level-1 record forms, asarf_dims.out_bytes_max for the size).  Replaces main.cc:233-327:
  * ConvertErsImSamplesToComplex (FBAQ4 records: ConvertAsarImBlocksToComplex) +
  * RawDataCorrection + ZeroNaNs + CalculateDopplerCentroid +
  * RangeCompression + RangeDopplerAlgorithm + SubsetResultsAndReassembleMeta +
@@ -337,6 +358,17 @@ int asarf_convert_ers_samples(const uint8_t* d_raw, int32_t raw_line_bytes, int3
 int asarf_convert_asar_blocks(const uint8_t* d_raw, int32_t record_bytes, int32_t records, const uint16_t* d_swst,
                               int32_t min_swst, const float* d_lut_i, const float* d_lut_q, void* d_img,
                               int64_t img_stride, int32_t range_size, void* stream);
+/* ConditionResultsSLC (envisat_format/src/envisat_format_kernels.cu:28-61, 95-106): IMS MDS records
+ * from a complex image (x_size x y_size, x_stride complex per row): per row `record_header_bytes`
+ * zeros, then per pixel big-endian int16 I and Q of trunc(clamp(value * calibration)).
+ * d_dest receives y_size * (record_header_bytes + 4 * x_size) bytes. */
+int asarf_condition_slc(const void* d_img, int32_t x_size, int32_t y_size, int32_t x_stride,
+                        int32_t record_header_bytes, float calibration, void* d_dest, void* stream);
+/* ConditionResultsDetected (:63-93, 108-114): IMP MDS records from a float image
+ * [azimuth_size][range_size]: per row the zero header, then per pixel
+ * uint16(min(10 log10(value * calibration), 65535)), least significant byte first. */
+int asarf_condition_detected(const float* d_img, int32_t range_size, int32_t azimuth_size,
+                             int32_t record_header_bytes, float calibration, void* d_dest, void* stream);
 /* Fbaq4Index (envisat_format/include/envisat_parse_util.h:21): reconstruction-table index of
  * the 4-bit code `code` in a block with block id `block` (256 * level + block). */
 int32_t asarf_fbaq4_index(int32_t block, int32_t code);

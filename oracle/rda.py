@@ -162,6 +162,78 @@ def pad_image(data: np.ndarray, rg_pad: int, az_pad: int) -> np.ndarray:
     return img
 
 
+# --------------------------------------------------------------------------- level-1 records
+
+def condition_slc(img: np.ndarray, cal: float, hdr: int) -> np.ndarray:
+    """CalibrateClampToBigEndian (envisat_format/src/envisat_format_kernels.cu:28-61): per row
+    `hdr` zero bytes, then per complex pixel int16 I and Q of clamp(value * cal) truncated toward
+    zero (NaN converts to 0 on the device), each most significant byte first."""
+    y, x = img.shape
+    out = np.zeros((y, hdr + 4 * x), dtype=np.uint8)
+
+    def i16(v):
+        s = (v.astype(np.float32) * np.float32(cal)).astype(np.float32)
+        c = np.where(s > 32767, np.float32(32767), np.where(s < -32768, np.float32(-32768), s))
+        return np.where(np.isnan(c), 0, np.trunc(np.nan_to_num(c))).astype(np.int64)
+
+    i, q = i16(img.real), i16(img.imag)
+    pay = out[:, hdr:].reshape(y, x, 4)
+    pay[:, :, 0] = (i >> 8) & 0xFF
+    pay[:, :, 1] = i & 0xFF
+    pay[:, :, 2] = (q >> 8) & 0xFF
+    pay[:, :, 3] = q & 0xFF
+    return out
+
+
+def condition_detected(img: np.ndarray, cal: float, hdr: int) -> np.ndarray:
+    """CalibrateClampToBigEndianDetected (envisat_format/src/envisat_format_kernels.cu:63-93): per
+    row `hdr` zero bytes, then per pixel uint16(min(10 * log10f(value * cal), 65535)) truncated
+    toward zero (negative, -inf and NaN convert to 0 on the device), least significant byte
+    first.  log10 here is numpy's float32 one; CUDA's log10f may differ by an ulp, which moves a
+    value only where 10 log10 lands within an ulp of an integer."""
+    y, x = img.shape
+    out = np.zeros((y, hdr + 2 * x), dtype=np.uint8)
+    v = (img.astype(np.float32) * np.float32(cal)).astype(np.float32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        db = (np.float32(10) * np.log10(v)).astype(np.float32)
+    db = np.where(np.float32(65535) < db, np.float32(65535), db)
+    u = np.where(np.isnan(db) | (db <= 0), 0, np.trunc(np.nan_to_num(db, neginf=0.0))).astype(np.int64)
+    pay = out[:, hdr:].reshape(y, x, 2)
+    pay[:, :, 0] = u & 0xFF
+    pay[:, :, 1] = (u >> 8) & 0xFF
+    return out
+
+
+def _mean_dev(x: np.ndarray, y: np.ndarray):
+    """DevicePaddedImage::CalcMean / CalcStdDev (cuda_util/device_padded_image.cu:331-414) over
+    pairs (x, y), NaN pairs skipped, divided by the number of all pairs, float results."""
+    n = F32(x.size)
+    ok = ~(np.isnan(x) | np.isnan(y))
+    xd, yd = x[ok].astype(np.float64), y[ok].astype(np.float64)
+    mx, my = F32(F32(xd.sum()) / n), F32(F32(yd.sum()) / n)
+    dx = F32(((xd - np.float64(mx)) ** 2).sum())
+    dy = F32(((yd - np.float64(my)) ** 2).sum())
+    return mx, my, F32(np.sqrt(F32(dx / n))), F32(np.sqrt(F32(dy / n)))
+
+
+def product_statistics_ims(slc: np.ndarray, cal: float = 1.0) -> np.ndarray:
+    """CalculateStatistics (main_flow.cc:666-670) of the subset SLC, scaled as main.cc:384-390."""
+    mx, my, ex, ey = _mean_dev(slc.real.ravel(), slc.imag.ravel())
+    return np.array([mx, my, ex, ey], dtype=np.float64) * float(cal)
+
+
+def product_statistics_imp(detected: np.ndarray, slc: np.ndarray, cal: float = 1.0) -> np.ndarray:
+    """CalculateStatisticsImaged (main_flow.cc:672-676) as main.cc:327-342 calls it: the
+    ground-range floats are written over the start of the subset SLC's buffer and that buffer is
+    viewed as a complex image of the ground-range size, so its 2 N floats (N pixels) are the
+    N ground-range values followed by the SLC floats at positions N .. 2N - 1 of the buffer."""
+    n = detected.size
+    buf = np.concatenate([detected.astype(np.float32).ravel(), slc.astype(np.complex64).view(np.float32).ravel()[n:2 * n]])
+    mx, my, ex, ey = _mean_dev(buf[0::2], buf[1::2])
+    return np.array([F32((mx + my) / F32(2)), 0.0, F32((ex + ey) / F32(2)), 0.0], dtype=np.float64) * \
+        np.array([cal, 1.0, cal, 1.0])
+
+
 # --------------------------------------------------------------------------- stage 2: IQ correction
 
 @dataclass

@@ -128,7 +128,14 @@ typedef struct ref_outputs {
     double ms_after_decode;   // same, from the end of the raw decode (its H2D excluded)
     double ms_wall;           // host wall clock of the whole call
     char error[256];
+    // with ref_set_statistics(1): CalculateStatistics of the subset (main.cc:380) and
+    // CalculateStatisticsImaged of the ground-range buffer (main.cc:327-333), unscaled
+    double ims_stats[4];
+    double imp_stats[4];
 } ref_outputs;
+
+static int g_statistics = 0;
+void ref_set_statistics(int on) { g_statistics = on; }
 
 // Runs the reference chain; optional host dumps (NULL to skip):
 //   corrected [na][nr] complex (after RawDataCorrection + ZeroNaNs), rc [na][nk] complex,
@@ -265,6 +272,15 @@ int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_ra
         sub.InitExtPtr(cols, lines, cols, lines, d_workspace);
         d_workspace = az_img.ReleaseMemory();
         if (h_slc) CHECK_CUDA_ERR(cudaMemcpy(h_slc, sub.Data(), static_cast<size_t>(cols) * lines * 8, cudaMemcpyDeviceToHost));
+        if (g_statistics) {
+            // CalculateStatistics (main_flow.cc:666-670)
+            const auto m = sub.CalcMean();
+            const auto d = sub.CalcStdDev(m.x, m.y);
+            o->ims_stats[0] = m.x;
+            o->ims_stats[1] = m.y;
+            o->ims_stats[2] = d.x;
+            o->ims_stats[3] = d.y;
+        }
         // AssembleMetadataFrom(..., range_pixels_recalib = near): slant range of the new first sample
         meta.slant_range_first_sample = CalcSlantRange(meta, near);
         meta.img.range_size = cols;
@@ -280,6 +296,17 @@ int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_ra
                                       cudaMemcpyDeviceToHost));
         auto srgr_dest = sub.ReleaseMemory();
         SlantRangeToGroundRangeInterpolation(meta, d_workspace.GetAs<float>(), srgr_dest.GetAs<float>());
+        if (g_statistics) {
+            // main.cc:327-333: the ground-range buffer viewed as a complex image of its size
+            DevicePaddedImage stats_image;
+            stats_image.InitExtPtr(meta.img.range_size, meta.img.azimuth_size, meta.img.range_size,
+                                   meta.img.azimuth_size, srgr_dest);
+            const auto m = stats_image.CalcMean();
+            const auto d = stats_image.CalcStdDev(m.x, m.y);
+            o->imp_stats[0] = (m.x + m.y) / 2;
+            o->imp_stats[2] = (d.x + d.y) / 2;
+            srgr_dest = stats_image.ReleaseMemory();
+        }
         cudaEventRecord(e2);
         CHECK_CUDA_ERR(cudaEventSynchronize(e2));
         float ms0 = 0, ms1 = 0;
@@ -318,6 +345,49 @@ int ref_focus(const asarf_scene* s, const double vr_poly[3], const uint8_t* h_ra
     } catch (const std::exception& e) {
         std::snprintf(o->error, sizeof(o->error), "%s", e.what());
         return -2;
+    }
+}
+
+// The reference's level-1 record conditioning on host inputs: ConditionResultsSLC over a padded
+// complex image [y_size][x_stride] (XSize x_size) and ConditionResultsDetected over a float
+// image [azimuth_size][range_size]; the records are copied back.
+int ref_condition_slc(const float* h_img, int32_t x_size, int32_t y_size, int32_t x_stride, int32_t hdr, float cal,
+                      uint8_t* h_out) {
+    try {
+        const size_t in_bytes = sizeof(cufftComplex) * static_cast<size_t>(x_stride) * y_size;
+        const size_t out_bytes = static_cast<size_t>(y_size) * (static_cast<size_t>(hdr) + 4ull * x_size);
+        CudaWorkspace ws(in_bytes);
+        CHECK_CUDA_ERR(cudaMemcpy(ws.Get(), h_img, in_bytes, cudaMemcpyHostToDevice));
+        DevicePaddedImage img;
+        img.InitExtPtr(x_size, y_size, x_stride, y_size, ws);
+        char* d_out = nullptr;
+        CHECK_CUDA_ERR(cudaMalloc(&d_out, out_bytes));
+        alus::asar::envformat::ConditionResultsSLC(img, d_out, hdr, cal);
+        CHECK_CUDA_ERR(cudaMemcpy(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost));
+        CHECK_CUDA_ERR(cudaFree(d_out));
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_condition_detected(const float* h_img, int32_t range_size, int32_t azimuth_size, int32_t hdr, float cal,
+                           uint8_t* h_out) {
+    try {
+        const size_t in_bytes = sizeof(float) * static_cast<size_t>(range_size) * azimuth_size;
+        const size_t out_bytes = static_cast<size_t>(azimuth_size) * (static_cast<size_t>(hdr) + 2ull * range_size);
+        float* d_in = nullptr;
+        char* d_out = nullptr;
+        CHECK_CUDA_ERR(cudaMalloc(&d_in, in_bytes));
+        CHECK_CUDA_ERR(cudaMalloc(&d_out, out_bytes));
+        CHECK_CUDA_ERR(cudaMemcpy(d_in, h_img, in_bytes, cudaMemcpyHostToDevice));
+        alus::asar::envformat::ConditionResultsDetected(d_in, d_out, range_size, azimuth_size, hdr, cal);
+        CHECK_CUDA_ERR(cudaMemcpy(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost));
+        CHECK_CUDA_ERR(cudaFree(d_in));
+        CHECK_CUDA_ERR(cudaFree(d_out));
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
     }
 }
 

@@ -22,7 +22,7 @@ class RefOutputs(C.Structure):
         ("grsr_poly", C.c_double * 5), ("first_line", C.c_int32), ("n_lines", C.c_int32),
         ("slc_cols", C.c_int32), ("out_rows", C.c_int32), ("out_cols", C.c_int32), ("max_aperture", C.c_int32),
         ("ms_total", C.c_double), ("ms_after_decode", C.c_double), ("ms_wall", C.c_double),
-        ("error", C.c_char * 256),
+        ("error", C.c_char * 256), ("ims_stats", C.c_double * 4), ("imp_stats", C.c_double * 4),
     ]
 
 
@@ -47,8 +47,45 @@ def load(path: Path = REF_LIB):
             g.restype = C.c_int
             g.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                           C.c_void_p]
+        for name in ("ref_condition_slc", "ref_condition_detected"):
+            if hasattr(lib, name):
+                h = getattr(lib, name)
+                h.restype = C.c_int
+                h.argtypes = [C.c_void_p, C.c_int32, C.c_int32] + ([C.c_int32] if name == "ref_condition_slc" else []) \
+                    + [C.c_int32, C.c_float, C.c_void_p]
+        if hasattr(lib, "ref_set_statistics"):
+            lib.ref_set_statistics.restype = None
+            lib.ref_set_statistics.argtypes = [C.c_int]
         _libs[path] = lib
     return _libs[path]
+
+
+def set_statistics(on: bool, lib_path: Path = REF_LIB) -> None:
+    """Have ref_focus also compute the product statistics main.cc writes (ims_stats, imp_stats)."""
+    load(lib_path).ref_set_statistics(int(bool(on)))
+
+
+def ref_condition_slc(img: np.ndarray, x_size: int, hdr: int, cal: float, lib_path: Path = REF_LIB) -> np.ndarray:
+    """The reference's ConditionResultsSLC on a complex64 [rows, stride] image (XSize x_size):
+    uint8 [rows, hdr + 4 x_size]."""
+    lib = load(lib_path)
+    img = np.ascontiguousarray(img, dtype=np.complex64)
+    y, stride = img.shape
+    out = np.empty((y, hdr + 4 * x_size), dtype=np.uint8)
+    if lib.ref_condition_slc(img.ctypes.data, x_size, y, stride, hdr, cal, out.ctypes.data) != 0:
+        raise RuntimeError("reference ConditionResultsSLC failed")
+    return out
+
+
+def ref_condition_detected(img: np.ndarray, hdr: int, cal: float, lib_path: Path = REF_LIB) -> np.ndarray:
+    """The reference's ConditionResultsDetected on a float32 [rows, cols] image: uint8 [rows, hdr + 2 cols]."""
+    lib = load(lib_path)
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    y, x = img.shape
+    out = np.empty((y, hdr + 2 * x), dtype=np.uint8)
+    if lib.ref_condition_detected(img.ctypes.data, x, y, hdr, cal, out.ctypes.data) != 0:
+        raise RuntimeError("reference ConditionResultsDetected failed")
+    return out
 
 
 def ref_convert_asar(raw: np.ndarray, swst, i_lut: np.ndarray, q_lut: np.ndarray, range_size: int,
@@ -95,7 +132,8 @@ def ref_focus(scene_c, vr_poly, raw: np.ndarray, swst=None, dumps: bool = False,
                        out.ctypes.data, cap, C.byref(o), *ptrs, d_raw_ptr or None)
     if rc != 0:
         raise RuntimeError(f"reference chain failed ({rc}): {o.error.decode(errors='replace')}")
-    res = {f: (list(getattr(o, f)) if f in ("dc_poly", "grsr_poly") else getattr(o, f)) for f, _ in o._fields_}
+    res = {f: (list(getattr(o, f)) if f in ("dc_poly", "grsr_poly", "ims_stats", "imp_stats") else getattr(o, f))
+           for f, _ in o._fields_}
     det = out[: o.out_rows * o.out_cols].reshape(o.out_rows, o.out_cols)
     if dumps:
         d["slc"] = d["slc"][: o.n_lines * o.slc_cols].reshape(o.n_lines, o.slc_cols)
