@@ -924,7 +924,9 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
         } else {
             // Windowed sinc at off - i, off = shift - walk + 8 in [7.5, 8.5]:
             // sin(pi (off - i)) = (-1)^i sin(pi off), and the common factor sin(pi off) / pi
-            // cancels in the normalised sum, leaving weights (-1)^i W_i / (off - i).
+            // cancels in the normalised sum, leaving weights (-1)^i W_i / (off - i).  The two end
+            // taps are skipped: their window values W_0 = W_15 = -1.4e-17 (a numpy.blackman
+            // rounding residue of an exact zero) give terms below half an ulp of every sum.
             const float off = fadd_rn(fsub_rn(shift, static_cast<float>(walk)), static_cast<float>(kRcmcTaps / 2));
             if (off == static_cast<float>(kRcmcTaps / 2)) {
                 out = srow[first + kRcmcTaps / 2];  // integer shift: sinc is a unit impulse
@@ -932,7 +934,7 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
                 constexpr float kWin[kRcmcTaps] = ASARF_BLACKMAN16;
                 float si = 0.0f, sq = 0.0f, nrm = 0.0f;
 #pragma unroll
-                for (int i = 0; i < kRcmcTaps; ++i) {
+                for (int i = 1; i < kRcmcTaps - 1; ++i) {
                     const float wgt = ((i & 1) ? -kWin[i] : kWin[i]) * rcp_approx(fsub_rn(off, static_cast<float>(i)));
                     const float2 d = srow[first + i];
                     si = fma_rn(d.x, wgt, si);

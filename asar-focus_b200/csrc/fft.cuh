@@ -54,26 +54,74 @@ ASARF_HD ASARF_INLINE float2 mul_mi(float2 a) {
     return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
+// ----------------------------------------------------------------------------- packed complex ops
+// Component-wise complex arithmetic: on sm_100 one f32x2 instruction per complex add, subtract,
+// real scaling or real multiply-add (the instruction issue rate, not the FMA pipe, bounds the
+// FFT kernels); the host emulation performs the same IEEE operations one lane at a time.
+ASARF_HD ASARF_INLINE float2 padd(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__)
+    return __fadd2_rn(a, b);
+#else
+    return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+
+// a - b, as b * (-1) + a (one rounding of the exact difference)
+ASARF_HD ASARF_INLINE float2 psub(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__)
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+#else
+    return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+
+ASARF_HD ASARF_INLINE float2 pscale(float2 a, float c) {
+#if defined(__CUDA_ARCH__)
+    return __fmul2_rn(a, make_float2(c, c));
+#else
+    return make_float2(a.x * c, a.y * c);
+#endif
+}
+
+// a * c + b
+ASARF_HD ASARF_INLINE float2 pfma(float2 a, float c, float2 b) {
+#if defined(__CUDA_ARCH__)
+    return __ffma2_rn(a, make_float2(c, c), b);
+#else
+    return make_float2(__builtin_fmaf(a.x, c, b.x), __builtin_fmaf(a.y, c, b.y));
+#endif
+}
+
+// r + mul_mi(p) and r - mul_mi(p): the swap of p's parts folded into two scalar adds
+template <bool INV>
+ASARF_HD ASARF_INLINE float2 add_mi(float2 r, float2 p) {
+    return INV ? make_float2(r.x - p.y, r.y + p.x) : make_float2(r.x + p.y, r.y - p.x);
+}
+template <bool INV>
+ASARF_HD ASARF_INLINE float2 sub_mi(float2 r, float2 p) {
+    return INV ? make_float2(r.x + p.y, r.y - p.x) : make_float2(r.x - p.y, r.y + p.x);
+}
+
 // ----------------------------------------------------------------------------- small DFTs
 // Sign convention: forward y_k = sum_m x_m exp(-2 pi i m k / R), inverse uses +.
 
 template <bool INV>
 ASARF_HD ASARF_INLINE void dft2(float2* v) {
-    float2 a = v[0];
-    v[0] = cadd(a, v[1]);
-    v[1] = csub(a, v[1]);
+    const float2 a = v[0];
+    v[0] = padd(a, v[1]);
+    v[1] = psub(a, v[1]);
 }
 
 template <bool INV>
 ASARF_HD ASARF_INLINE void dft4(float2* v) {
-    float2 t0 = cadd(v[0], v[2]);
-    float2 t1 = csub(v[0], v[2]);
-    float2 t2 = cadd(v[1], v[3]);
-    float2 t3 = mul_mi<INV>(csub(v[1], v[3]));
-    v[0] = cadd(t0, t2);
-    v[2] = csub(t0, t2);
-    v[1] = cadd(t1, t3);
-    v[3] = csub(t1, t3);
+    const float2 t0 = padd(v[0], v[2]);
+    const float2 t1 = psub(v[0], v[2]);
+    const float2 t2 = padd(v[1], v[3]);
+    const float2 d = psub(v[1], v[3]);
+    v[0] = padd(t0, t2);
+    v[2] = psub(t0, t2);
+    v[1] = add_mi<INV>(t1, d);
+    v[3] = sub_mi<INV>(t1, d);
 }
 
 template <bool INV>
@@ -84,49 +132,48 @@ ASARF_HD ASARF_INLINE void dft8(float2* v) {
     dft4<INV>(e);
     dft4<INV>(o);
     // o_k *= W8^k (forward W8 = exp(-i pi/4))
-    float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
-                    : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
-    float2 o2 = mul_mi<INV>(o[2]);
-    float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
-                    : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
-    v[0] = cadd(e[0], o[0]);
-    v[4] = csub(e[0], o[0]);
-    v[1] = cadd(e[1], o1);
-    v[5] = csub(e[1], o1);
-    v[2] = cadd(e[2], o2);
-    v[6] = csub(e[2], o2);
-    v[3] = cadd(e[3], o3);
-    v[7] = csub(e[3], o3);
+    const float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                          : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    const float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                          : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    v[0] = padd(e[0], o[0]);
+    v[4] = psub(e[0], o[0]);
+    v[1] = padd(e[1], o1);
+    v[5] = psub(e[1], o1);
+    v[2] = add_mi<INV>(e[2], o[2]);
+    v[6] = sub_mi<INV>(e[2], o[2]);
+    v[3] = padd(e[3], o3);
+    v[7] = psub(e[3], o3);
 }
 
 template <bool INV>
 ASARF_HD ASARF_INLINE void dft3(float2* v) {
     constexpr float s3 = 0.8660254037844387f;
-    float2 a = cadd(v[1], v[2]);
-    float2 b = csub(v[1], v[2]);
-    float2 t = make_float2(v[0].x - 0.5f * a.x, v[0].y - 0.5f * a.y);
-    float2 u = mul_mi<INV>(cscale(b, s3));
-    v[0] = cadd(v[0], a);
-    v[1] = cadd(t, u);
-    v[2] = csub(t, u);
+    const float2 a = padd(v[1], v[2]);
+    const float2 b = psub(v[1], v[2]);
+    const float2 t = pfma(a, -0.5f, v[0]);
+    const float2 bs = pscale(b, s3);
+    v[0] = padd(v[0], a);
+    v[1] = add_mi<INV>(t, bs);
+    v[2] = sub_mi<INV>(t, bs);
 }
 
 template <bool INV>
 ASARF_HD ASARF_INLINE void dft5(float2* v) {
     constexpr float c1 = 0.30901699437494745f, s1 = 0.9510565162951535f;
     constexpr float c2 = -0.8090169943749473f, s2 = 0.5877852522924732f;
-    float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
-    float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
-    float2 x0 = v[0];
-    float2 r1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
-    float2 r2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
-    float2 i1 = mul_mi<INV>(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
-    float2 i2 = mul_mi<INV>(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
-    v[0] = make_float2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
-    v[1] = cadd(r1, i1);
-    v[4] = csub(r1, i1);
-    v[2] = cadd(r2, i2);
-    v[3] = csub(r2, i2);
+    const float2 a1 = padd(v[1], v[4]), b1 = psub(v[1], v[4]);
+    const float2 a2 = padd(v[2], v[3]), b2 = psub(v[2], v[3]);
+    const float2 x0 = v[0];
+    const float2 r1 = pfma(a2, c2, pfma(a1, c1, x0));
+    const float2 r2 = pfma(a2, c1, pfma(a1, c2, x0));
+    const float2 p1 = pfma(b2, s2, pscale(b1, s1));
+    const float2 p2 = pfma(b2, -s1, pscale(b1, s2));
+    v[0] = padd(padd(x0, a1), a2);
+    v[1] = add_mi<INV>(r1, p1);
+    v[4] = sub_mi<INV>(r1, p1);
+    v[2] = add_mi<INV>(r2, p2);
+    v[3] = sub_mi<INV>(r2, p2);
 }
 
 template <bool INV>
@@ -134,25 +181,25 @@ ASARF_HD ASARF_INLINE void dft7(float2* v) {
     constexpr float c1 = 0.6234898018587336f, s1 = 0.7818314824680298f;
     constexpr float c2 = -0.22252093395631434f, s2 = 0.9749279121818236f;
     constexpr float c3 = -0.900968867902419f, s3 = 0.43388373911755823f;
-    float2 a1 = cadd(v[1], v[6]), b1 = csub(v[1], v[6]);
-    float2 a2 = cadd(v[2], v[5]), b2 = csub(v[2], v[5]);
-    float2 a3 = cadd(v[3], v[4]), b3 = csub(v[3], v[4]);
-    float2 x0 = v[0];
+    const float2 a1 = padd(v[1], v[6]), b1 = psub(v[1], v[6]);
+    const float2 a2 = padd(v[2], v[5]), b2 = psub(v[2], v[5]);
+    const float2 a3 = padd(v[3], v[4]), b3 = psub(v[3], v[4]);
+    const float2 x0 = v[0];
     // k = 1..3: cos(2 pi m k / 7) pattern over m = 1..3; sin pattern with sign folding
-    float2 r1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x + c3 * a3.x, x0.y + c1 * a1.y + c2 * a2.y + c3 * a3.y);
-    float2 r2 = make_float2(x0.x + c2 * a1.x + c3 * a2.x + c1 * a3.x, x0.y + c2 * a1.y + c3 * a2.y + c1 * a3.y);
-    float2 r3 = make_float2(x0.x + c3 * a1.x + c1 * a2.x + c2 * a3.x, x0.y + c3 * a1.y + c1 * a2.y + c2 * a3.y);
+    const float2 r1 = pfma(a3, c3, pfma(a2, c2, pfma(a1, c1, x0)));
+    const float2 r2 = pfma(a3, c1, pfma(a2, c3, pfma(a1, c2, x0)));
+    const float2 r3 = pfma(a3, c2, pfma(a2, c1, pfma(a1, c3, x0)));
     // sin(2 pi m k / 7): k=1: s1 s2 s3 ; k=2: s2 -s3 -s1 ; k=3: s3 -s1 s2
-    float2 i1 = mul_mi<INV>(make_float2(s1 * b1.x + s2 * b2.x + s3 * b3.x, s1 * b1.y + s2 * b2.y + s3 * b3.y));
-    float2 i2 = mul_mi<INV>(make_float2(s2 * b1.x - s3 * b2.x - s1 * b3.x, s2 * b1.y - s3 * b2.y - s1 * b3.y));
-    float2 i3 = mul_mi<INV>(make_float2(s3 * b1.x - s1 * b2.x + s2 * b3.x, s3 * b1.y - s1 * b2.y + s2 * b3.y));
-    v[0] = make_float2(x0.x + a1.x + a2.x + a3.x, x0.y + a1.y + a2.y + a3.y);
-    v[1] = cadd(r1, i1);
-    v[6] = csub(r1, i1);
-    v[2] = cadd(r2, i2);
-    v[5] = csub(r2, i2);
-    v[3] = cadd(r3, i3);
-    v[4] = csub(r3, i3);
+    const float2 p1 = pfma(b3, s3, pfma(b2, s2, pscale(b1, s1)));
+    const float2 p2 = pfma(b3, -s1, pfma(b2, -s3, pscale(b1, s2)));
+    const float2 p3 = pfma(b3, s2, pfma(b2, -s1, pscale(b1, s3)));
+    v[0] = padd(padd(padd(x0, a1), a2), a3);
+    v[1] = add_mi<INV>(r1, p1);
+    v[6] = sub_mi<INV>(r1, p1);
+    v[2] = add_mi<INV>(r2, p2);
+    v[5] = sub_mi<INV>(r2, p2);
+    v[3] = add_mi<INV>(r3, p3);
+    v[4] = sub_mi<INV>(r3, p3);
 }
 
 template <int R, bool INV>
