@@ -824,7 +824,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
     }
     ASARF_SYNC();
     if (!a.inverse) {
-        fft_forward_pairs(a.plan1, s, xt, xt, tid, nthr);
+        fft_forward_pairs<true>(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
             const int x = x0 + c;
@@ -836,7 +836,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
             s[t] = cmulc(s[t], tw[k1]);
         }
         ASARF_SYNC();
-        fft_inverse_dif_pairs(a.plan1, s, xt, xt, tid, nthr);
+        fft_inverse_dif_pairs<true>(a.plan1, s, xt, xt, tid, nthr);
         const int lo = a.state ? a.state->first_line : 0;
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {

@@ -311,7 +311,8 @@ ASARF_HD ASARF_INLINE void dft_composite(float2* v) {
 // Any radix the schedules use: the direct small DFTs, or a composite of two of them.
 template <int R, bool INV>
 ASARF_HD ASARF_INLINE void dft_any(float2* v) {
-    if constexpr (R == 12) dft_composite<4, 3, INV>(v);
+    if constexpr (R == 9) dft_composite<3, 3, INV>(v);
+    else if constexpr (R == 12) dft_composite<4, 3, INV>(v);
     else if constexpr (R == 16) dft_composite<4, 4, INV>(v);
     else if constexpr (R == 24) dft_composite<8, 3, INV>(v);
     else if constexpr (R == 32) dft_composite<8, 4, INV>(v);
@@ -453,13 +454,23 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
     }
 }
 
-// Column-pair stages take the prime-power radices only: a composite radix holds twice its
+// Column-pair stages take the prime-power radices: a larger composite radix holds twice its
 // length in registers per column pair, which lifts the azimuth kernels from 64 to 128
 // registers per thread and halves their resident CTAs (measured slower despite fewer passes).
-template <bool INV, bool TW_FIRST>
+// NINE adds radix 9 (two radix-3 DFTs in registers, 36 values per column pair: 71 registers
+// in the strided kernel, whose occupancy shared memory limits anyway) for plans that merge
+// factors 3 * 3; it is compiled only where such plans run, since every extra case costs the
+// other kernels registers.
+template <bool INV, bool TW_FIRST, bool NINE = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int npair,
                                                    const FastDiv& pdiv, int ldc, const float2* __restrict__ tw,
                                                    int tid, int nthr) {
+    if constexpr (NINE) {
+        if (R == 9) {
+            fft_stage_pair<9, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr);
+            return;
+        }
+    }
     switch (R) {
         case 2: fft_stage_pair<2, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
         case 3: fft_stage_pair<3, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
@@ -471,12 +482,13 @@ ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int 
 }
 
 // Column-pair forms of fft_forward / fft_inverse / fft_inverse_dif (ncol and ldc even).
+template <bool NINE = false>
 ASARF_HD ASARF_INLINE void fft_forward_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
     for (int i = 0; i < p.nst; ++i) {
-        fft_stage_pair_dispatch<false, false>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
-                                              nthr);
+        fft_stage_pair_dispatch<false, false, NINE>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw,
+                                                    tid, nthr);
         ASARF_SYNC();
     }
 }
@@ -491,12 +503,13 @@ ASARF_HD ASARF_INLINE void fft_inverse_pairs(const FftPlan& p, float2* s, int nc
     }
 }
 
+template <bool NINE = false>
 ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
     for (int i = 0; i < p.nst; ++i) {
-        fft_stage_pair_dispatch<true, false>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
-                                             nthr);
+        fft_stage_pair_dispatch<true, false, NINE>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw,
+                                                   tid, nthr);
         ASARF_SYNC();
     }
 }

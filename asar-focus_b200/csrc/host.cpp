@@ -312,6 +312,23 @@ int32_t fft_size_above(int32_t v) {
 
 bool build_fft(int n, HostFft& h) { return build_fft_radices(n, factorize(n), h); }
 
+std::vector<int> strided_radices(int n) {
+    // the default factors with each pair of 3s merged into a 9 (first, so that the short
+    // radices run on the shortest spans)
+    std::vector<int> rest, out;
+    int threes = 0;
+    for (int r : factorize(n)) {
+        if (r == 3)
+            ++threes;
+        else
+            rest.push_back(r);
+    }
+    for (int k = 0; k < threes / 2; ++k) out.push_back(9);
+    out.insert(out.end(), rest.begin(), rest.end());
+    if (threes & 1) out.push_back(3);
+    return out;
+}
+
 bool build_fft_radices(int n, const std::vector<int>& f, HostFft& h) {
     long long prod = 1;
     for (int r : f) prod *= r;
@@ -532,7 +549,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     const int n_ctr = ct_radices(p->rc_len, ctr);
     const bool rc_ok = n_ctr ? build_fft_radices(p->rc_len, std::vector<int>(ctr, ctr + n_ctr), p->rc)
                              : build_fft(p->rc_len, p->rc);
-    if (!rc_ok || !build_fft(p->n1, p->f1) || !build_fft(p->n2, p->f2) || !build_fft(p->az_pad, p->fN)) {
+    if (!rc_ok || !build_fft_radices(p->n1, strided_radices(p->n1), p->f1) || !build_fft(p->n2, p->f2) || !build_fft(p->az_pad, p->fN)) {
         delete p;
         return set_error(ASARF_ERR_INVALID, "FFT schedule failed");
     }

@@ -26,6 +26,8 @@ int srgr_poly(const asarf_scene& s, double slant_first, int range_size, int azim
 bool build_fft(int n, HostFft& h);
 // Same with an explicit radix sequence (product n), e.g. a compile-time schedule's.
 bool build_fft_radices(int n, const std::vector<int>& radices, HostFft& h);
+// radices of the strided azimuth pass: pairs of 3s merged into radix 9
+std::vector<int> strided_radices(int n);
 int choose_rc_len(int nr);
 int32_t fft_size_above(int32_t v);
 void matched_filter_table(const std::complex<float>* chirp, int nc, const HostFft& fft, std::vector<float2>& mf);

@@ -287,7 +287,7 @@ int asarf_range_doppler(const asarf_rda_params* prm, void* d_src, void* d_out, i
         if (N % d == 0) n2 = d;
     const int n1 = N / n2;
     HostFft f1, f2, fN;
-    if (n2 < 2 || !build_fft(n1, f1) || !build_fft(n2, f2) || !build_fft(N, fN))
+    if (n2 < 2 || !build_fft_radices(n1, strided_radices(n1), f1) || !build_fft(n2, f2) || !build_fft(N, fN))
         return set_error(ASARF_ERR_INVALID, "range_doppler: azimuth size %d is not 2^a3^b5^c7^d", N);
     // tables + a finalised state carrying the Doppler polynomial
     DevBuf tw1(sizeof(float2) * n1), dr1(sizeof(int) * n1), tw2(sizeof(float2) * n2), dr2(sizeof(int) * n2),

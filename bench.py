@@ -383,12 +383,16 @@ def run_reference(args, rank: int, world: int) -> None:
         e2e.append(r["ms_wall"])
     clocks = sampler.stop()
     samples = sc.range_size * sc.azimuth_size
-    ms = statistics.mean(dev_ms)
+    # median per step: the reference allocates and synchronises inside every call, so a single
+    # host-side stall (e.g. a page-mapping of a fresh allocation) would skew a mean of a few steps
+    # against it; the median is the generous reading for the reference
+    ms = statistics.median(dev_ms)
     value = samples / ms / 1e3
-    e2e_ms = statistics.mean(e2e)
+    e2e_ms = statistics.median(e2e)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "ms_statistic": "median of steps",
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (cuFFT)", "data": "synthetic",
         "config": {"workload": f"{args.workload}: ERS-like {sc.range_size} range x {sc.azimuth_size} azimuth "
                                f"(same seeded scene as the optimised arm)",

@@ -57,6 +57,20 @@ def test_negative_doppler_window_variant(emu_lib):
     _check(plan, out, res, ref)
 
 
+def tiny_nine(**kw):
+    """The small scene on 1200 lines: azimuth FFT 1215 = 45 x 27, strided pass [9, 5]."""
+    base = dict(azimuth_size=1200, seed=13)
+    base.update(kw)
+    return S.tiny(**base)
+
+
+def test_strided_radix_nine_matches_oracle(emu_lib):
+    sc, raw, _ = scene_and_raw(emu_lib, tiny_nine)
+    plan, out, res = _run(emu_lib, sc, raw)
+    assert plan.dims["n1"] == 45
+    _check(plan, out, res, oracle_focus(sc, raw))
+
+
 def test_range_fft_length_does_not_matter(emu_lib):
     """Any range FFT length >= range size gives the same compressed samples."""
     sc, raw, _ = scene_and_raw(emu_lib, S.tiny)

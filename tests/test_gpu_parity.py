@@ -38,7 +38,14 @@ def asar_small(**kw):
     return S.asar_im(**base)
 
 
-@pytest.mark.parametrize("factory", [S.tiny, S.ers_small, asar_small])
+def tiny_nine(**kw):
+    """The small scene on 1200 lines: azimuth FFT 1215 = 45 x 27, strided pass radices [9, 5]."""
+    base = dict(azimuth_size=1200, seed=13)
+    base.update(kw)
+    return S.tiny(**base)
+
+
+@pytest.mark.parametrize("factory", [S.tiny, S.ers_small, asar_small, tiny_nine])
 def test_matches_oracle(gpu_lib, factory):
     sc, raw, _ = scene_and_raw(gpu_lib, factory)
     plan, out, res = _focus(gpu_lib, sc, raw)
