@@ -919,7 +919,7 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
     float2 out = make_float2(0.0f, 0.0f);
     if (!(calc_x - kRcmcTaps / 2 < 0 || calc_x + kRcmcTaps / 2 >= a.nk)) {
         const int first = cs + walk - kRcmcTaps / 2;  // smem column of tap 0
-        if (first < 0 || first + kRcmcTaps > a.wt) {
+        if (first + 1 < 0 || first + kRcmcTaps - 1 > a.wt) {
             atomic_or_u32(err_flag, kErrRcmcHalo);
         } else {
             // Windowed sinc at off - i, off = shift - walk + 8 in [7.5, 8.5]:
@@ -932,18 +932,18 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
                 out = srow[first + kRcmcTaps / 2];  // integer shift: sinc is a unit impulse
             } else {
                 constexpr float kWin[kRcmcTaps] = ASARF_BLACKMAN16;
-                float si = 0.0f, sq = 0.0f, nrm = 0.0f;
+                float2 acc = make_float2(0.0f, 0.0f);
+                float nrm = 0.0f;
 #pragma unroll
                 for (int i = 1; i < kRcmcTaps - 1; ++i) {
                     const float wgt = ((i & 1) ? -kWin[i] : kWin[i]) * rcp_approx(fsub_rn(off, static_cast<float>(i)));
                     const float2 d = srow[first + i];
-                    si = fma_rn(d.x, wgt, si);
-                    sq = fma_rn(d.y, wgt, sq);
+                    acc = pfma(d, wgt, acc);
                     nrm = fadd_rn(nrm, wgt);
                 }
                 if (nrm != 0.0f) {
                     const float inv = rcp_approx(nrm);
-                    out = make_float2(fmul_rn(si, inv), fmul_rn(sq, inv));
+                    out = make_float2(fmul_rn(acc.x, inv), fmul_rn(acc.y, inv));
                 }
             }
         }
@@ -972,6 +972,22 @@ ASARF_HD ASARF_INLINE void az_rd_tables(const AzRdArgs& a, int tile, int k1, int
 inline size_t az_rd_smem(int n2, int wt, int xt) {
     return sizeof(float2) * static_cast<size_t>(n2) * wt + sizeof(ColParams) * static_cast<size_t>(xt) +
            sizeof(int) * static_cast<size_t>(n2) + 16;
+}
+
+// Right range halo of the range-Doppler block: the taps used (1 .. 14 of 16) reach 6 columns
+// right of the integer walk, which is at most ceil of the largest walk (the left halo is the
+// 8 columns of tap 0, kept whole so that the tile's TMA start stays 16-byte aligned).
+inline int rcmc_right_halo(double max_walk) { return kRcmcTaps / 2 - 1 + static_cast<int>(std::ceil(max_walk)); }
+
+// Range-tile width of the range-Doppler block: the widest even width <= 64 whose block leaves
+// room for two resident blocks per SM (2 x 512 threads at 64 registers fill the register file;
+// 228 KB of shared memory per SM, 1 KB reserved per block).  With one block per SM the
+// block-wide barriers of the FFT stages leave the SM idle (measured 2.63 -> 1.92 ms at n2 = 168).
+constexpr size_t kAzRdTwoBlockSmem = 228 * 1024 / 2 - 1024 - 256;
+inline int az_rd_tile_width(int n2, int hl, int hr) {
+    int xt = 64;
+    while (xt > 16 && az_rd_smem(n2, xt + hl + hr, xt) > kAzRdTwoBlockSmem) xt -= 2;
+    return xt;
 }
 
 ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s,

@@ -573,12 +573,12 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         const double f = s.prf;
         const double walk = s.wavelength * s.wavelength * f * f * rmax / (8 * vr_min * vr_min) / s.range_spacing;
         p->hl = kRcmcTaps / 2;
-        p->hr = kRcmcTaps / 2 + static_cast<int>(std::ceil(walk)) + 2;
-        if ((64 + p->hl + p->hr) & 1) ++p->hr;  // even tile width: TMA rows are whole 16-byte units
+        p->hr = rcmc_right_halo(walk);
+        if ((p->hl + p->hr) & 1) ++p->hr;  // even tile width: TMA rows are whole 16-byte units
     }
     p->pitch = (p->nk + 31) / 32 * 32;
     p->xt1 = (p->n1 * 32 * 8 <= 160 * 1024) ? 32 : 16;
-    p->xt2 = 64;
+    p->xt2 = az_rd_tile_width(p->n2, p->hl, p->hr);
 
     // chirp matched filter in the forward transform's output order, scaled by 1/L
     std::vector<std::complex<float>> chirp;

@@ -353,10 +353,10 @@ int asarf_range_doppler(const asarf_rda_params* prm, void* d_src, void* d_out, i
     d.plan2 = f2.plan;
     d.drev2 = dr2.as<int>();
     d.nk = x_size;
-    d.xt = 64;
     d.hl = kRcmcTaps / 2;
-    d.hr = kRcmcTaps / 2 + static_cast<int>(std::ceil(walk)) + 2;
-    if ((d.xt + d.hl + d.hr) & 1) ++d.hr;  // column-pair transforms need an even tile width
+    d.hr = rcmc_right_halo(walk);
+    if ((d.hl + d.hr) & 1) ++d.hr;  // column-pair transforms need an even tile width
+    d.xt = az_rd_tile_width(n2, d.hl, d.hr);
     d.wt = d.xt + d.hl + d.hr;
     d.prf = static_cast<float>(prm->prf);
     d.bin_step = d.prf / static_cast<float>(N);
