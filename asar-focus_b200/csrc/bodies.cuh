@@ -1013,13 +1013,16 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
 #if defined(__CUDA_ARCH__)
     {
         const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+        // a lane's two column records stay in registers for all rows (read from shared memory
+        // per sample, the 48-byte records cost 4-way bank conflicts on every field)
+        const ColParams cp0 = cps[lane < a.xt ? lane : 0], cp1 = cps[lane + 32 < a.xt ? lane + 32 : 0];
         for (int p = warp; p < n2; p += nwarps) {
             const int f = fbin[p];
             const float2* srow = s + p * wt;
             float2 v0 = make_float2(0.0f, 0.0f), v1 = make_float2(0.0f, 0.0f);
             const int c0 = lane, c1 = lane + 32;
-            if (c0 < a.xt && x0 + c0 < a.nk) v0 = rcmc_mf_sample(a, cps[c0], x0 + c0, f, srow, a.hl + c0, err_flag);
-            if (c1 < a.xt && x0 + c1 < a.nk) v1 = rcmc_mf_sample(a, cps[c1], x0 + c1, f, srow, a.hl + c1, err_flag);
+            if (c0 < a.xt && x0 + c0 < a.nk) v0 = rcmc_mf_sample(a, cp0, x0 + c0, f, srow, a.hl + c0, err_flag);
+            if (c1 < a.xt && x0 + c1 < a.nk) v1 = rcmc_mf_sample(a, cp1, x0 + c1, f, srow, a.hl + c1, err_flag);
             __syncwarp();
             if (c0 < a.xt) s[p * wt + a.hl + c0] = v0;
             if (c1 < a.xt) s[p * wt + a.hl + c1] = v1;
