@@ -831,12 +831,8 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
             if (x < a.nk) a.out[static_cast<long long>(rowmap[p]) * a.pitch + x] = cmul(s[t], tw[p]);
         }
     } else {
-        for (int t = tid; t < n1 * xt; t += nthr) {
-            const int k1 = static_cast<int>(fdiv_u(t, dxt));
-            s[t] = cmulc(s[t], tw[k1]);
-        }
-        ASARF_SYNC();
-        fft_inverse_dif_pairs<true>(a.plan1, s, xt, xt, tid, nthr);
+        // conj(twiddle) of row k1 applied as the first stage loads the row
+        fft_inverse_dif_pairs<true>(a.plan1, s, xt, xt, tid, nthr, tw);
         const int lo = a.state ? a.state->first_line : 0;
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {

@@ -406,9 +406,12 @@ ASARF_HD ASARF_INLINE void fft_stage_dif_inv(float2* s, int n, int S, const Fast
 // both columns' samples and one twiddle set serves both butterflies.  Needs ldc even, the
 // tile base 16-byte aligned and an even column count.  TW_FIRST selects decimation in time
 // (twiddle, then DFT); INV selects the inverse DFT sign and conjugated twiddles.
-template <int R, bool INV, bool TW_FIRST>
+// PRE: the loaded values of row l are first multiplied by conj(pre[l]) (a per-row table, here the
+// input twiddles of the inverse strided pass), saving a separate pass over the tile.
+template <int R, bool INV, bool TW_FIRST, bool PRE = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv& sdiv, int npair, const FastDiv& pdiv,
-                                          int ldc, const float2* __restrict__ tw, int tid, int nthr) {
+                                          int ldc, const float2* __restrict__ tw, int tid, int nthr,
+                                          const float2* pre = nullptr) {
     const int M = S * R;
     const int items = (n / R) * npair;
     const int tw_step = n / M;
@@ -425,6 +428,11 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
             const float4 q = p[m * st];
             u[m] = make_float2(q.x, q.y);
             v[m] = make_float2(q.z, q.w);
+            if constexpr (PRE) {
+                const float2 w = pre[b * M + j + m * S];
+                u[m] = cmulc(u[m], w);
+                v[m] = cmulc(v[m], w);
+            }
         }
         // W_M^{j q}: one table load, higher powers by recurrence (error ~ q ulp); a table load
         // per q is exact but measured slower
@@ -461,23 +469,23 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
 // in the strided kernel, whose occupancy shared memory limits anyway) for plans that merge
 // factors 3 * 3; it is compiled only where such plans run, since every extra case costs the
 // other kernels registers.
-template <bool INV, bool TW_FIRST, bool NINE = false>
+template <bool INV, bool TW_FIRST, bool NINE = false, bool PRE = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int npair,
                                                    const FastDiv& pdiv, int ldc, const float2* __restrict__ tw,
-                                                   int tid, int nthr) {
+                                                   int tid, int nthr, const float2* pre = nullptr) {
     if constexpr (NINE) {
         if (R == 9) {
-            fft_stage_pair<9, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr);
+            fft_stage_pair<9, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre);
             return;
         }
     }
     switch (R) {
-        case 2: fft_stage_pair<2, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
-        case 3: fft_stage_pair<3, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
-        case 4: fft_stage_pair<4, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
-        case 5: fft_stage_pair<5, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
-        case 7: fft_stage_pair<7, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
-        default: fft_stage_pair<8, INV, TW_FIRST>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr); break;
+        case 2: fft_stage_pair<2, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
+        case 3: fft_stage_pair<3, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
+        case 4: fft_stage_pair<4, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
+        case 5: fft_stage_pair<5, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
+        case 7: fft_stage_pair<7, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
+        default: fft_stage_pair<8, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
     }
 }
 
@@ -503,13 +511,19 @@ ASARF_HD ASARF_INLINE void fft_inverse_pairs(const FftPlan& p, float2* s, int nc
     }
 }
 
+// pre (optional): per-row table whose conjugate multiplies the input (folded into stage 0).
 template <bool NINE = false>
-ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr,
+                                                 const float2* pre = nullptr) {
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
     for (int i = 0; i < p.nst; ++i) {
-        fft_stage_pair_dispatch<true, false, NINE>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw,
-                                                   tid, nthr);
+        if (i == 0 && pre)
+            fft_stage_pair_dispatch<true, false, NINE, true>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv,
+                                                             ldc, p.tw, tid, nthr, pre);
+        else
+            fft_stage_pair_dispatch<true, false, NINE>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc,
+                                                       p.tw, tid, nthr);
         ASARF_SYNC();
     }
 }
