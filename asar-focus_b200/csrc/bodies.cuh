@@ -802,6 +802,17 @@ ASARF_HD ASARF_INLINE void az_strided_tables(const AzStridedArgs& a, int b, int 
     }
 }
 
+// Store of a column pair (u at column x, v at x + 1) of one output row: one 16-byte store when
+// both columns exist and the address allows it.
+ASARF_HD ASARF_INLINE void store_pair(float2* dst, int x, int nk, float2 u, float2 v) {
+    if (x + 1 < nk && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+        *reinterpret_cast<float4*>(dst) = make_float4(u.x, u.y, v.x, v.y);
+    } else {
+        dst[0] = u;
+        if (x + 1 < nk) dst[1] = v;
+    }
+}
+
 ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int b, int tid, int nthr, float2* s,
                                            const float2* tw, const int* rowmap, bool preloaded) {
     const int x0 = tile * a.xt;
@@ -824,6 +835,8 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
     }
     ASARF_SYNC();
     if (!a.inverse) {
+        // (writing the last stage straight to HBM, as the range-Doppler block does, measured
+        // slower here: its rows scatter through the digit-reversed row map)
         fft_forward_pairs<true>(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
@@ -986,12 +999,23 @@ inline int az_rd_tile_width(int n2, int hl, int hr) {
     return xt;
 }
 
+// Epilogue of the range-Doppler block: row r of the inverse transform, column pair cp.
+struct AzRdOut {
+    static constexpr bool kActive = true;
+    const AzRdArgs* a;
+    int x0, k1;
+    ASARF_HD ASARF_INLINE void operator()(int r, int cp, float2 u, float2 v) const {
+        const int x = x0 + 2 * cp;
+        if (x >= a->nk) return;
+        store_pair(a->out + static_cast<long long>(k1 * a->n2 + r) * a->pitch + x, x, a->nk, u, v);
+    }
+};
+
 ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s,
                                       const ColParams* cps, const int* fbin, unsigned int* err_flag, bool preloaded) {
     const int x0 = tile * a.xt;
     const int n2 = a.n2, wt = a.wt;
     const FastDiv dwt = make_fastdiv(static_cast<unsigned int>(wt));
-    const FastDiv dxt = make_fastdiv(static_cast<unsigned int>(a.xt));
     if (!preloaded) {
         for (int t = tid; t < n2 * wt; t += nthr) {
             const int r = static_cast<int>(fdiv_u(t, dwt)), c = t - r * wt;
@@ -1038,12 +1062,8 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
         }
     }
 #endif
-    fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr);
-    for (int t = tid; t < n2 * a.xt; t += nthr) {
-        const int r = static_cast<int>(fdiv_u(t, dxt)), c = t - r * a.xt;
-        const int x = x0 + c;
-        if (x < a.nk) a.out[static_cast<long long>(k1 * n2 + r) * a.pitch + x] = s[r * wt + a.hl + c];
-    }
+    // the inverse transform's last stage stores the block's rows k1 * n2 + r directly
+    fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr, AzRdOut{&a, x0, k1});
 }
 
 // ----------------------------------------------------------------------------- L1 product records

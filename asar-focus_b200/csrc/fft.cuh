@@ -406,12 +406,19 @@ ASARF_HD ASARF_INLINE void fft_stage_dif_inv(float2* s, int n, int S, const Fast
 // both columns' samples and one twiddle set serves both butterflies.  Needs ldc even, the
 // tile base 16-byte aligned and an even column count.  TW_FIRST selects decimation in time
 // (twiddle, then DFT); INV selects the inverse DFT sign and conjugated twiddles.
+// Epilogue of a column-pair transform: the last stage hands each output (row l, column pair
+// cp) to epi(l, cp, u, v) instead of storing it back to the tile.
+struct NoEpi {
+    static constexpr bool kActive = false;
+    ASARF_HD ASARF_INLINE void operator()(int, int, float2, float2) const {}
+};
+
 // PRE: the loaded values of row l are first multiplied by conj(pre[l]) (a per-row table, here the
 // input twiddles of the inverse strided pass), saving a separate pass over the tile.
-template <int R, bool INV, bool TW_FIRST, bool PRE = false>
+template <int R, bool INV, bool TW_FIRST, bool PRE = false, class Epi = NoEpi>
 ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv& sdiv, int npair, const FastDiv& pdiv,
                                           int ldc, const float2* __restrict__ tw, int tid, int nthr,
-                                          const float2* pre = nullptr) {
+                                          const float2* pre = nullptr, const Epi& epi = Epi()) {
     const int M = S * R;
     const int items = (n / R) * npair;
     const int tw_step = n / M;
@@ -457,8 +464,13 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
                 w = cmul(w, w1);
             }
         }
+        if constexpr (Epi::kActive) {
 #pragma unroll
-        for (int m = 0; m < R; ++m) p[m * st] = make_float4(u[m].x, u[m].y, v[m].x, v[m].y);
+            for (int m = 0; m < R; ++m) epi(b * M + j + m * S, cp, u[m], v[m]);
+        } else {
+#pragma unroll
+            for (int m = 0; m < R; ++m) p[m * st] = make_float4(u[m].x, u[m].y, v[m].x, v[m].y);
+        }
     }
 }
 
@@ -469,24 +481,27 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
 // in the strided kernel, whose occupancy shared memory limits anyway) for plans that merge
 // factors 3 * 3; it is compiled only where such plans run, since every extra case costs the
 // other kernels registers.
-template <bool INV, bool TW_FIRST, bool NINE = false, bool PRE = false>
+template <bool INV, bool TW_FIRST, bool NINE = false, bool PRE = false, class Epi = NoEpi>
 ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int npair,
                                                    const FastDiv& pdiv, int ldc, const float2* __restrict__ tw,
-                                                   int tid, int nthr, const float2* pre = nullptr) {
+                                                   int tid, int nthr, const float2* pre = nullptr,
+                                                   const Epi& epi = Epi()) {
+#define ASARF_PAIR(RR) fft_stage_pair<RR, INV, TW_FIRST, PRE, Epi>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre, epi)
     if constexpr (NINE) {
         if (R == 9) {
-            fft_stage_pair<9, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre);
+            ASARF_PAIR(9);
             return;
         }
     }
     switch (R) {
-        case 2: fft_stage_pair<2, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
-        case 3: fft_stage_pair<3, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
-        case 4: fft_stage_pair<4, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
-        case 5: fft_stage_pair<5, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
-        case 7: fft_stage_pair<7, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
-        default: fft_stage_pair<8, INV, TW_FIRST, PRE>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre); break;
+        case 2: ASARF_PAIR(2); break;
+        case 3: ASARF_PAIR(3); break;
+        case 4: ASARF_PAIR(4); break;
+        case 5: ASARF_PAIR(5); break;
+        case 7: ASARF_PAIR(7); break;
+        default: ASARF_PAIR(8); break;
     }
+#undef ASARF_PAIR
 }
 
 // Column-pair forms of fft_forward / fft_inverse / fft_inverse_dif (ncol and ldc even).
@@ -501,12 +516,19 @@ ASARF_HD ASARF_INLINE void fft_forward_pairs(const FftPlan& p, float2* s, int nc
     }
 }
 
-ASARF_HD ASARF_INLINE void fft_inverse_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
+// With an active epilogue the last stage writes through it and the tile is left unfinished.
+template <class Epi = NoEpi>
+ASARF_HD ASARF_INLINE void fft_inverse_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr,
+                                             const Epi& epi = Epi()) {
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
     for (int i = p.nst - 1; i >= 0; --i) {
-        fft_stage_pair_dispatch<true, true>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
-                                            nthr);
+        if (Epi::kActive && i == 0)
+            fft_stage_pair_dispatch<true, true, false, false, Epi>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair,
+                                                                   pdiv, ldc, p.tw, tid, nthr, nullptr, epi);
+        else
+            fft_stage_pair_dispatch<true, true>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
+                                                nthr);
         ASARF_SYNC();
     }
 }
