@@ -753,6 +753,16 @@ ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y
     for (int l = tid; l < a.nk; l += nthr) orow[l] = s[l];
 }
 
+// Compressed line store of the compile-time transform: sample x < nk to orow[x].
+struct RcOut {
+    static constexpr bool kActive = true;
+    float2* orow;
+    int nk;
+    ASARF_HD ASARF_INLINE void operator()(int x, float2 v) const {
+        if (x < nk) orow[x] = v;
+    }
+};
+
 // Same transform with a compile-time schedule (lengths in kCtLengths): all loops unrolled,
 // all index arithmetic constant.
 template <int L, int FMT = kRawErsBytes>
@@ -772,13 +782,8 @@ ASARF_HD ASARF_INLINE void range_compress_ct_body(const RangeCompressArgs& a, in
             }
         },
         tid);
-    ct_fft_mf_ifft<L>(s, a.ctw, a.mf, tid);
-    float2* orow = a.out + static_cast<long long>(y) * a.out_pitch;
-    ct_phase<NTHR>(
-        [&](int t) {
-            for (int l = t; l < a.nk; l += NTHR) orow[l] = s[ct_pad<L>(l)];
-        },
-        tid);
+    // the last inverse pass stores the kept samples x < Nk of the line directly
+    ct_fft_mf_ifft<L>(s, a.ctw, a.mf, tid, RcOut{a.out + static_cast<long long>(y) * a.out_pitch, a.nk});
 }
 
 // ----------------------------------------------------------------------------- azimuth strided pass

@@ -100,11 +100,11 @@ inline int ct_smem_elems_of(int L) {
 
 // Run `phase(tid)` for this thread and barrier (device), or for every thread in turn (host
 // emulation, where a phase must complete for all threads before the next one starts).
-template <int NTHR, class F>
+template <int NTHR, bool SYNC = true, class F>
 ASARF_HD ASARF_INLINE void ct_phase(F&& phase, int tid) {
 #if defined(__CUDA_ARCH__)
     phase(tid);
-    __syncthreads();
+    if (SYNC) __syncthreads();
 #else
     (void)tid;
     for (int t = 0; t < NTHR; ++t) phase(t);
@@ -113,8 +113,10 @@ ASARF_HD ASARF_INLINE void ct_phase(F&& phase, int tid) {
 
 // One pass I < count-1 (span S > 1, a multiple of Q): forward DIF (DFT, then twiddle output q
 // by W_M^{jq}) or inverse DIT (conjugate twiddles on the inputs, then the inverse DFT).
-template <int L, int I, bool INV>
-ASARF_HD ASARF_INLINE void ct_pass(float2* s, const float2* __restrict__ ctw, int t) {
+// An active Epi receives each output (natural position, value) instead of the tile: the last
+// inverse pass hands the line straight to its destination.
+template <int L, int I, bool INV, class Epi = NoEpi>
+ASARF_HD ASARF_INLINE void ct_pass(float2* s, const float2* __restrict__ ctw, int t, const Epi& epi = Epi{}) {
     constexpr int NTHR = CtSchedule<L>::nthr;
     constexpr int R = CtSchedule<L>::r[I];
     constexpr int S = ct_span<L, I>();
@@ -148,8 +150,13 @@ ASARF_HD ASARF_INLINE void ct_pass(float2* s, const float2* __restrict__ ctw, in
                 for (int q = 1; q < R; ++q) v[q] = cmul(v[q], ASARF_LDG(ctw + TWO + (q - 1) * S + j));
             }
         }
+        if constexpr (Epi::kActive) {
 #pragma unroll
-        for (int m = 0; m < R; ++m) p[m * STRIDE] = v[m];
+            for (int m = 0; m < R; ++m) epi(b * M + j + m * S, v[m]);
+        } else {
+#pragma unroll
+            for (int m = 0; m < R; ++m) p[m * STRIDE] = v[m];
+        }
     }
 }
 
@@ -179,17 +186,19 @@ ASARF_HD ASARF_INLINE void ct_middle(float2* s, const float2* __restrict__ mf, i
 }
 
 // Forward transform, matched filter, inverse transform of the padded tile s (natural order
-// in, natural order out, unscaled); every pass ends with a barrier.
-template <int L>
+// in, unscaled); the last pass hands its outputs to epi (natural position, value) and ends
+// without a barrier, every other pass ends with one.
+template <int L, class Epi>
 ASARF_HD ASARF_INLINE void ct_fft_mf_ifft(float2* s, const float2* __restrict__ ctw, const float2* __restrict__ mf,
-                                          int tid) {
+                                          int tid, const Epi& epi) {
     constexpr int NTHR = CtSchedule<L>::nthr;
     static_assert(CtSchedule<L>::count == 3, "three-pass schedules");
+    static_assert(Epi::kActive, "the last pass writes through its epilogue");
     ct_phase<NTHR>([&](int t) { ct_pass<L, 0, false>(s, ctw, t); }, tid);
     ct_phase<NTHR>([&](int t) { ct_pass<L, 1, false>(s, ctw, t); }, tid);
     ct_phase<NTHR>([&](int t) { ct_middle<L>(s, mf, t); }, tid);
     ct_phase<NTHR>([&](int t) { ct_pass<L, 1, true>(s, ctw, t); }, tid);
-    ct_phase<NTHR>([&](int t) { ct_pass<L, 0, true>(s, ctw, t); }, tid);
+    ct_phase<NTHR, false>([&](int t) { ct_pass<L, 0, true>(s, ctw, t, epi); }, tid);
 }
 
 }  // namespace asarf
