@@ -842,7 +842,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
     if (!a.inverse) {
         // (writing the last stage straight to HBM, as the range-Doppler block does, measured
         // slower here: its rows scatter through the digit-reversed row map)
-        fft_forward_pairs<true>(a.plan1, s, xt, xt, tid, nthr);
+        fft_forward_pairs<true, true>(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
             const int x = x0 + c;
@@ -850,7 +850,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
         }
     } else {
         // conj(twiddle) of row k1 applied as the first stage loads the row
-        fft_inverse_dif_pairs<true>(a.plan1, s, xt, xt, tid, nthr, tw);
+        fft_inverse_dif_pairs<true, true>(a.plan1, s, xt, xt, tid, nthr, tw);
         const int lo = a.state ? a.state->first_line : 0;
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {
@@ -941,20 +941,28 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
             // cancels in the normalised sum, leaving weights (-1)^i W_i / (off - i).  The two end
             // taps are skipped: their window values W_0 = W_15 = -1.4e-17 (a numpy.blackman
             // rounding residue of an exact zero) give terms below half an ulp of every sum.
+            // With dl = off - 8 (exact) a weight is 1 / fma(dl, c_i, (8 - i) c_i), c_i = (-1)^i / W_i
+            // (constants): one FMA and one reciprocal per tap, within 2 ulp of the quotient since
+            // |8 - i| >= 1 wherever the constant term is not zero.  The normaliser sums in pairs.
             const float off = fadd_rn(fsub_rn(shift, static_cast<float>(walk)), static_cast<float>(kRcmcTaps / 2));
-            if (off == static_cast<float>(kRcmcTaps / 2)) {
+            const float dl = fsub_rn(off, static_cast<float>(kRcmcTaps / 2));
+            if (dl == 0.0f) {
                 out = srow[first + kRcmcTaps / 2];  // integer shift: sinc is a unit impulse
             } else {
                 constexpr float kWin[kRcmcTaps] = ASARF_BLACKMAN16;
                 float2 acc = make_float2(0.0f, 0.0f);
-                float nrm = 0.0f;
+                float2 nrm2 = make_float2(0.0f, 0.0f);
 #pragma unroll
-                for (int i = 1; i < kRcmcTaps - 1; ++i) {
-                    const float wgt = ((i & 1) ? -kWin[i] : kWin[i]) * rcp_approx(fsub_rn(off, static_cast<float>(i)));
-                    const float2 d = srow[first + i];
-                    acc = pfma(d, wgt, acc);
-                    nrm = fadd_rn(nrm, wgt);
+                for (int i = 1; i < kRcmcTaps - 1; i += 2) {
+                    const float ca = -1.0f / kWin[i];  // i odd
+                    const float cb = 1.0f / kWin[i + 1];
+                    const float wa = rcp_approx(fma_rn(dl, ca, static_cast<float>(kRcmcTaps / 2 - i) * ca));
+                    const float wb = rcp_approx(fma_rn(dl, cb, static_cast<float>(kRcmcTaps / 2 - i - 1) * cb));
+                    acc = pfma(srow[first + i], wa, acc);
+                    acc = pfma(srow[first + i + 1], wb, acc);
+                    nrm2 = padd(nrm2, make_float2(wa, wb));
                 }
+                const float nrm = fadd_rn(nrm2.x, nrm2.y);
                 if (nrm != 0.0f) {
                     const float inv = rcp_approx(nrm);
                     out = make_float2(fmul_rn(acc.x, inv), fmul_rn(acc.y, inv));

@@ -413,9 +413,41 @@ struct NoEpi {
     ASARF_HD ASARF_INLINE void operator()(int, int, float2, float2) const {}
 };
 
+// u * w from w and iw = i w: u.x w + u.y iw, two packed operations.
+ASARF_HD ASARF_INLINE float2 cmul_rot(float2 u, float2 w, float2 iw) { return pfma(iw, u.y, pscale(w, u.x)); }
+ASARF_HD ASARF_INLINE float2 rot90(float2 w) { return make_float2(-w.y, w.x); }
+
+// Value q of both columns times W^q (INV: conj(W)^q), W = w1, q = 1 .. R-1.  PTW: packed
+// products (one rotation of each power serves both columns); otherwise scalar complex products.
+template <int R, bool INV, bool PTW>
+ASARF_HD ASARF_INLINE void pair_twiddle(float2* u, float2* v, float2 w1) {
+    if constexpr (PTW) {
+        const float2 ws = INV ? make_float2(w1.x, -w1.y) : w1;
+        const float2 is = rot90(ws);
+        float2 w = ws, iw = is;
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+            u[q] = cmul_rot(u[q], w, iw);
+            v[q] = cmul_rot(v[q], w, iw);
+            if (q + 1 < R) {
+                w = cmul_rot(w, ws, is);
+                iw = rot90(w);
+            }
+        }
+    } else {
+        float2 w = w1;
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+            u[q] = INV ? cmulc(u[q], w) : cmul(u[q], w);
+            v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
+            w = cmul(w, w1);
+        }
+    }
+}
+
 // PRE: the loaded values of row l are first multiplied by conj(pre[l]) (a per-row table, here the
 // input twiddles of the inverse strided pass), saving a separate pass over the tile.
-template <int R, bool INV, bool TW_FIRST, bool PRE = false, class Epi = NoEpi>
+template <int R, bool INV, bool TW_FIRST, bool PRE = false, class Epi = NoEpi, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv& sdiv, int npair, const FastDiv& pdiv,
                                           int ldc, const float2* __restrict__ tw, int tid, int nthr,
                                           const float2* pre = nullptr, const Epi& epi = Epi()) {
@@ -444,26 +476,10 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
         // W_M^{j q}: one table load, higher powers by recurrence (error ~ q ulp); a table load
         // per q is exact but measured slower
         const float2 w1 = j != 0 ? ASARF_LDG(tw + j * tw_step) : make_float2(1.0f, 0.0f);
-        if (TW_FIRST && j != 0) {
-            float2 w = w1;
-#pragma unroll
-            for (int q = 1; q < R; ++q) {
-                u[q] = INV ? cmulc(u[q], w) : cmul(u[q], w);
-                v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
-                w = cmul(w, w1);
-            }
-        }
+        if (TW_FIRST && j != 0) pair_twiddle<R, INV, PTW>(u, v, w1);
         dft_any<R, INV>(u);
         dft_any<R, INV>(v);
-        if (!TW_FIRST && j != 0) {
-            float2 w = w1;
-#pragma unroll
-            for (int q = 1; q < R; ++q) {
-                u[q] = INV ? cmulc(u[q], w) : cmul(u[q], w);
-                v[q] = INV ? cmulc(v[q], w) : cmul(v[q], w);
-                w = cmul(w, w1);
-            }
-        }
+        if (!TW_FIRST && j != 0) pair_twiddle<R, INV, PTW>(u, v, w1);
         if constexpr (Epi::kActive) {
 #pragma unroll
             for (int m = 0; m < R; ++m) epi(b * M + j + m * S, cp, u[m], v[m]);
@@ -480,13 +496,15 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
 // NINE adds radix 9 (two radix-3 DFTs in registers, 36 values per column pair: 71 registers
 // in the strided kernel, whose occupancy shared memory limits anyway) for plans that merge
 // factors 3 * 3; it is compiled only where such plans run, since every extra case costs the
-// other kernels registers.
-template <bool INV, bool TW_FIRST, bool NINE = false, bool PRE = false, class Epi = NoEpi>
+// other kernels registers.  PTW selects the packed twiddle products (measured faster in the
+// strided kernel, slower in the range-Doppler block at its 64-register bound).
+template <bool INV, bool TW_FIRST, bool NINE = false, bool PRE = false, class Epi = NoEpi, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int npair,
                                                    const FastDiv& pdiv, int ldc, const float2* __restrict__ tw,
                                                    int tid, int nthr, const float2* pre = nullptr,
                                                    const Epi& epi = Epi()) {
-#define ASARF_PAIR(RR) fft_stage_pair<RR, INV, TW_FIRST, PRE, Epi>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre, epi)
+#define ASARF_PAIR(RR) \
+    fft_stage_pair<RR, INV, TW_FIRST, PRE, Epi, PTW>(s, n, S, sdiv, npair, pdiv, ldc, tw, tid, nthr, pre, epi)
     if constexpr (NINE) {
         if (R == 9) {
             ASARF_PAIR(9);
@@ -505,13 +523,13 @@ ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int 
 }
 
 // Column-pair forms of fft_forward / fft_inverse / fft_inverse_dif (ncol and ldc even).
-template <bool NINE = false>
+template <bool NINE = false, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_forward_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr) {
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
     for (int i = 0; i < p.nst; ++i) {
-        fft_stage_pair_dispatch<false, false, NINE>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw,
-                                                    tid, nthr);
+        fft_stage_pair_dispatch<false, false, NINE, false, NoEpi, PTW>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair,
+                                                                      pdiv, ldc, p.tw, tid, nthr);
         ASARF_SYNC();
     }
 }
@@ -534,18 +552,18 @@ ASARF_HD ASARF_INLINE void fft_inverse_pairs(const FftPlan& p, float2* s, int nc
 }
 
 // pre (optional): per-row table whose conjugate multiplies the input (folded into stage 0).
-template <bool NINE = false>
+template <bool NINE = false, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr,
                                                  const float2* pre = nullptr) {
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
     for (int i = 0; i < p.nst; ++i) {
         if (i == 0 && pre)
-            fft_stage_pair_dispatch<true, false, NINE, true>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv,
-                                                             ldc, p.tw, tid, nthr, pre);
+            fft_stage_pair_dispatch<true, false, NINE, true, NoEpi, PTW>(p.radix[i], s, p.n, p.span[i], p.sdiv[i],
+                                                                        npair, pdiv, ldc, p.tw, tid, nthr, pre);
         else
-            fft_stage_pair_dispatch<true, false, NINE>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc,
-                                                       p.tw, tid, nthr);
+            fft_stage_pair_dispatch<true, false, NINE, false, NoEpi, PTW>(p.radix[i], s, p.n, p.span[i], p.sdiv[i],
+                                                                         npair, pdiv, ldc, p.tw, tid, nthr);
         ASARF_SYNC();
     }
 }
