@@ -1169,29 +1169,61 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
     const int r_hi = e0 > e1 ? e0 : e1;
     // each input row is read once and added to whichever box mean(s) contain it, in row
     // order, so both sums accumulate exactly as the reference's two loops do
-    for (int c = tid; c < a.nx; c += nthr) {
-        float sum0 = 0.0f, sum1 = 0.0f;
-        for (int r = r_lo; r < r_hi; ++r) {
-            const float2 v = base[static_cast<long long>(r) * a.pitch + c];
-            const float p2 = fma_rn(v.x, v.x, fmul_rn(v.y, v.y));
-            if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
-            if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
+    // the window spans at most kTailRows rows (5, or 6 where x + 3 rounds up across a power
+    // of two); all of a column's rows are loaded before any is summed, two columns at a time
+    constexpr int kTailRows = 6;
+    const int nr = r_hi - r_lo;
+    // the box divisions and the resampling index divide by block constants: correctly rounded
+    // quotients from their correctly rounded reciprocals (div_by_recip_rn)
+    const float fc0 = c0 ? static_cast<float>(c0) : 1.0f, fc1 = c1 ? static_cast<float>(c1) : 1.0f;
+    const float rc0 = fdiv_rn(1.0f, fc0), rc1 = fdiv_rn(1.0f, fc1);
+    for (int cb = tid; cb < a.nx; cb += 2 * nthr) {
+        float2 v[2][kTailRows];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c = cb + h * nthr;
+#pragma unroll
+            for (int k = 0; k < kTailRows; ++k) {
+                v[h][k] = make_float2(0.0f, 0.0f);
+                if (k < nr && c < a.nx) v[h][k] = base[static_cast<long long>(r_lo + k) * a.pitch + c];
+            }
         }
-        if (c0) sum0 = fdiv_rn(sum0, static_cast<float>(c0));
-        if (c1) sum1 = fdiv_rn(sum1, static_cast<float>(c1));
-        float val = 0.0f;
-        if (c0 && c1) val = fma_rn(fsub_rn(sum1, sum0), mu, sum0);
-        ml[c] = fmul_rn(val, ASARF_LDG(tv.rsl + c));
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c = cb + h * nthr;
+            if (c >= a.nx) break;
+            float sum0 = 0.0f, sum1 = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kTailRows; ++k) {
+                const int r = r_lo + k;
+                if (k >= nr) break;
+                const float p2 = fma_rn(v[h][k].x, v[h][k].x, fmul_rn(v[h][k].y, v[h][k].y));
+                if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
+                if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
+            }
+            for (int r = r_lo + kTailRows; r < r_hi; ++r) {
+                const float2 w = base[static_cast<long long>(r) * a.pitch + c];
+                const float p2 = fma_rn(w.x, w.x, fmul_rn(w.y, w.y));
+                if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
+                if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
+            }
+            if (c0) sum0 = div_by_recip_rn(sum0, fc0, rc0);
+            if (c1) sum1 = div_by_recip_rn(sum1, fc1, rc1);
+            float val = 0.0f;
+            if (c0 && c1) val = fma_rn(fsub_rn(sum1, sum0), mu, sum0);
+            ml[c] = fmul_rn(val, ASARF_LDG(tv.rsl + c));
+        }
     }
     ASARF_SYNC();
     float* orow = a.mds ? nullptr : a.out + static_cast<long long>(y) * a.out_pitch;
     uint8_t* rec = a.mds ? a.mds + static_cast<long long>(y) * (a.mds_hdr + 2 * tv.ng) : nullptr;
     if (rec)
         for (int i = tid; i < a.mds_hdr; i += nthr) rec[i] = 0;
+    const float rsp = fdiv_rn(1.0f, a.range_spacing);
     for (int xg = tid; xg < tv.ng; xg += nthr) {
         const float gd = fmul_rn(static_cast<float>(xg), a.ground_spacing);
         const float rd = polyval_f32(tv.grsr, gd);
-        const float idx = fdiv_rn(rd, a.range_spacing);
+        const float idx = div_by_recip_rn(rd, a.range_spacing, rsp);
         int i0 = static_cast<int>(idx);
         const float dx = fsub_rn(idx, static_cast<float>(i0));
         if (i0 < 0 || i0 + 1 >= a.nx) {

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
     az_rd_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, a.use_tma != 0);
 }
 
-__global__ void __launch_bounds__(512) k_tail(TailArgs a, unsigned int* err) {
+__global__ void __launch_bounds__(512, 2) k_tail(TailArgs a, unsigned int* err) {
     extern __shared__ float smem_tail[];
     tail_body(a, blockIdx.x, threadIdx.x, blockDim.x, smem_tail, err);
 }
