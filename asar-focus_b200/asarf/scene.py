@@ -341,8 +341,16 @@ def ers_mid(**kw) -> Scene:
     return ers_full(**base)
 
 
+def asar_fbaq_mid(**kw) -> Scene:
+    """5616 x 8192 cut of the FBAQ4 scene: profiling case (complex images above L2)."""
+    base = dict(name="asar_fbaq_mid", azimuth_size=8192)
+    base.update(kw)
+    return asar_fbaq(**base)
+
+
 WORKLOADS = {"ers_small": ers_small, "ers_full": ers_full, "asar_im": asar_im, "asar_strip": asar_strip,
-             "tiny": tiny, "ers_mid": ers_mid, "asar_fbaq": asar_fbaq, "tiny_fbaq": tiny_fbaq}
+             "tiny": tiny, "ers_mid": ers_mid, "asar_fbaq": asar_fbaq, "tiny_fbaq": tiny_fbaq,
+             "asar_fbaq_mid": asar_fbaq_mid}
 
 
 def with_sizes(sc: Scene, **kw) -> Scene:
