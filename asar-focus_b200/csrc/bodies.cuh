@@ -588,18 +588,25 @@ ASARF_HD ASARF_INLINE void stats_fold_body(const RawStatsArgs& a, int tiles_y, i
 // cuda_util/device_padded_image.cu:331-414), the Doppler centroid per range block and its
 // quadratic fit (sar/fractional_doppler_centroid.cu:98-139), and the results-window choice
 // that depends on the sign of the fitted constant term (main_flow.cc:155-178).
-ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
+// Constants of the corrected-sample map z = (p*I + p0, u*Q + v*I + w) and the statistics
+// error bits, shared by the IQ part and the per-block Doppler part of the finalisation.
+struct FinalizeMap {
+    double p, p0, u, v, w, pad_mag2;
+    unsigned int err;
+};
+
+// IQ statistics and the correction constants; the FocusState fields are written when st is set.
+ASARF_HD inline FinalizeMap finalize_stats(const FinalizeArgs& a, FocusState* st) {
     const StatAccum& s = *a.acc;
-    FocusState& st = *a.state;
     const FloatStatAccum* fs = a.facc;
     auto mom = [&](int k) { return fs ? fs->mom[k] : static_cast<double>(s.mom[k]); };
-    auto lag = [&](int b, int q) { return fs ? fs->lag[b][q] : static_cast<double>(s.lag[b][q]); };
     const double n = mom(0);
     const double SI = mom(1), SQ = mom(2);
     const double SII = mom(3), SQQ = mom(4);
     const double SIQ = mom(5);
-    unsigned int err = 0;
-    if (n == 0.0) err |= kErrStatsEmpty;
+    FinalizeMap m;
+    m.err = 0;
+    if (n == 0.0) m.err |= kErrStatsEmpty;
     const float total = static_cast<float>(a.n_total);
     // mean: float(sum) / float(total)
     const float dc_i = static_cast<float>(SI) / total;
@@ -608,8 +615,6 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
     const double cii = SII - 2.0 * di * SI + n * di * di;  // sum over filled of (I - dc_i)^2
     const double cqq = SQQ - 2.0 * dq * SQ + n * dq * dq;
     const double ciq = SIQ - dq * SI - di * SQ + n * di * dq;
-    const float std_i = sqrtf(static_cast<float>(cii) / total);
-    const float std_q = sqrtf(static_cast<float>(cqq) / total);
     // padding samples hold 0 - dc after the DC step and enter the gain / phase sums
     const double npad = static_cast<double>(a.n_pad);
     const double i1sq = cii + npad * di * di;
@@ -621,50 +626,66 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
     const double delta = (i1q1 / gf) / (i1sq / (gf * gf));
     const float sin_c = static_cast<float>(delta);
     const float cos_c = static_cast<float>(1.0 - delta * delta);
-    st.dc_i = dc_i;
-    st.dc_q = dc_q;
-    st.gain = gain_f;
-    st.sin_c = sin_c;
-    st.cos_c = cos_c;
-    st.rgain = fdiv_rn(1.0f, gain_f);
-    st.rcos = fdiv_rn(1.0f, cos_c);
-    st.dc_i_d = dc_i;
-    st.dc_q_d = dc_q;
-    st.iq_gain = gain;
-    st.phase_error = 360.0 * asin(delta) / (2.0 * 3.14159265358979323846);
-    st.stddev_i = std_i;
-    st.stddev_q = std_q;
-
+    if (st) {
+        st->dc_i = dc_i;
+        st->dc_q = dc_q;
+        st->gain = gain_f;
+        st->sin_c = sin_c;
+        st->cos_c = cos_c;
+        st->rgain = fdiv_rn(1.0f, gain_f);
+        st->rcos = fdiv_rn(1.0f, cos_c);
+        st->dc_i_d = dc_i;
+        st->dc_q_d = dc_q;
+        st->iq_gain = gain;
+        st->phase_error = 360.0 * asin(delta) / (2.0 * 3.14159265358979323846);
+        st->stddev_i = sqrtf(static_cast<float>(cii) / total);
+        st->stddev_q = sqrtf(static_cast<float>(cqq) / total);
+    }
     // corrected sample z = (p*I + p0, u*Q + v*I + w)
-    const double p = 1.0 / gf, p0 = -di / gf;
+    m.p = 1.0 / gf;
+    m.p0 = -di / gf;
     const double sc = sin_c, cc = cos_c;
-    const double u = 1.0 / cc, v = -sc * p / cc, w = (-dq - sc * p0) / cc;
-    const double pad_mag2 = p0 * p0 + w * w;  // |corrected zero padding sample|^2
-    double xs[kMaxDcBlocks], ys[kMaxDcBlocks];
+    m.u = 1.0 / cc;
+    m.v = -sc * m.p / cc;
+    m.w = (-dq - sc * m.p0) / cc;
+    m.pad_mag2 = m.p0 * m.p0 + m.w * m.w;  // |corrected zero padding sample|^2
+    return m;
+}
+
+// Doppler centroid of range block b from its lag-1 sums through the correction map.
+ASARF_HD inline void finalize_block(const FinalizeArgs& a, const FinalizeMap& m, int b, double* xs, double* ys,
+                                    FocusState& st) {
+    const StatAccum& s = *a.acc;
+    const FloatStatAccum* fs = a.facc;
+    auto lag = [&](int q) { return fs ? fs->lag[b][q] : static_cast<double>(s.lag[b][q]); };
+    const double p = m.p, p0 = m.p0, u = m.u, v = m.v, w = m.w;
+    const double np = lag(0);
+    const double sA = lag(1), sB = lag(2);
+    const double sC = lag(3), sD = lag(4);
+    const double sAC = lag(5), sBD = lag(6);
+    const double sAD = lag(7), sBC = lag(8);
+    double re = p * p * sAC + p * p0 * (sA + sC) + p0 * p0 * np + u * u * sBD + u * v * (sBC + sAD) +
+                u * w * (sB + sD) + v * v * sAC + v * w * (sA + sC) + w * w * np;
+    const double im = p * u * (sAD - sBC) + p * w * (sA - sC) + p0 * u * (sD - sB) + p0 * v * (sC - sA);
+    const int xb = b * a.dc_step;
+    const int xe = xb + a.dc_step;
+    // columns of this block beyond the data lie in the range padding (constant rows)
+    int pad_lo = xb > a.nr ? xb : a.nr;
+    int pad_hi = xe < a.rg_stride ? xe : a.rg_stride;
+    // (only when the padding went through the correction, i.e. reference statistics)
+    if (a.n_pad > 0 && pad_hi > pad_lo) re += static_cast<double>(pad_hi - pad_lo) * (a.na - 1) * m.pad_mag2;
+    const double ang = atan2(im, re);
+    const double hz = a.prf * (ang / (2.0 * 3.14159265358979323846));
+    xs[b] = static_cast<double>((xb + xe) / 2);
+    ys[b] = hz;
+    st.dc_blk_hz[b] = hz;
+}
+
+// Doppler polynomial fit over the blocks, the DC-sign variant and the error bits.
+ASARF_HD inline void finalize_fit(const FinalizeArgs& a, FocusState& st, const double* xs, const double* ys,
+                                  unsigned int err) {
     const int nblk = a.nblk < kMaxDcBlocks ? a.nblk : kMaxDcBlocks;
     if (a.nblk > kMaxDcBlocks) err |= kErrDcBlocks;
-    for (int b = 0; b < nblk; ++b) {
-        const double np = lag(b, 0);
-        const double sA = lag(b, 1), sB = lag(b, 2);
-        const double sC = lag(b, 3), sD = lag(b, 4);
-        const double sAC = lag(b, 5), sBD = lag(b, 6);
-        const double sAD = lag(b, 7), sBC = lag(b, 8);
-        double re = p * p * sAC + p * p0 * (sA + sC) + p0 * p0 * np + u * u * sBD + u * v * (sBC + sAD) +
-                    u * w * (sB + sD) + v * v * sAC + v * w * (sA + sC) + w * w * np;
-        const double im = p * u * (sAD - sBC) + p * w * (sA - sC) + p0 * u * (sD - sB) + p0 * v * (sC - sA);
-        const int xb = b * a.dc_step;
-        const int xe = xb + a.dc_step;
-        // columns of this block beyond the data lie in the range padding (constant rows)
-        int pad_lo = xb > a.nr ? xb : a.nr;
-        int pad_hi = xe < a.rg_stride ? xe : a.rg_stride;
-        // (only when the padding went through the correction, i.e. reference statistics)
-        if (a.n_pad > 0 && pad_hi > pad_lo) re += static_cast<double>(pad_hi - pad_lo) * (a.na - 1) * pad_mag2;
-        const double ang = atan2(im, re);
-        const double hz = a.prf * (ang / (2.0 * 3.14159265358979323846));
-        xs[b] = static_cast<double>((xb + xe) / 2);
-        ys[b] = hz;
-        st.dc_blk_hz[b] = hz;
-    }
     st.nblk = nblk;
     double poly[3] = {0.0, 0.0, 0.0};
     polyfit_qr<kMaxDcBlocks, 3>(xs, ys, nblk, 2, poly);
@@ -681,6 +702,16 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
     st.first_line = a.first_line[st.variant];
     st.n_lines = a.n_lines[st.variant];
     st.errors = err;
+}
+
+// The whole finalisation on one thread.
+ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
+    FocusState& st = *a.state;
+    const FinalizeMap m = finalize_stats(a, &st);
+    double xs[kMaxDcBlocks], ys[kMaxDcBlocks];
+    const int nblk = a.nblk < kMaxDcBlocks ? a.nblk : kMaxDcBlocks;
+    for (int b = 0; b < nblk; ++b) finalize_block(a, m, b, xs, ys, st);
+    finalize_fit(a, st, xs, ys, m.err);
 }
 
 // ----------------------------------------------------------------------------- range compression

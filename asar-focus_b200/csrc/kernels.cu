@@ -48,8 +48,16 @@ __global__ void __launch_bounds__(256) k_condition(ConditionArgs a) {
     condition_row(a, blockIdx.x, threadIdx.x, blockDim.x);
 }
 
+// One warp: the Doppler blocks' angles (an FP64 atan2 each) lane-parallel, the fit on lane 0.
 __global__ void k_finalize(FinalizeArgs a) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) finalize_body(a);
+    __shared__ double xs[kMaxDcBlocks], ys[kMaxDcBlocks];
+    if (blockIdx.x != 0) return;
+    FocusState& st = *a.state;
+    const FinalizeMap m = finalize_stats(a, threadIdx.x == 0 ? &st : nullptr);
+    const int nblk = a.nblk < kMaxDcBlocks ? a.nblk : kMaxDcBlocks;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) finalize_block(a, m, b, xs, ys, st);
+    __syncthreads();
+    if (threadIdx.x == 0) finalize_fit(a, st, xs, ys, m.err);
 }
 
 // FBAQ4 record into shared memory: its 16-byte-aligned interior with vector loads, the
