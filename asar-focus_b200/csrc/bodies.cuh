@@ -140,6 +140,18 @@ ASARF_HD ASARF_INLINE unsigned int funnel_r(unsigned int lo, unsigned int hi, un
 #endif
 }
 
+// bytes of (x, y) = b0..b7 picked by the low 3 bits of each selector nibble (PRMT default mode)
+ASARF_HD ASARF_INLINE unsigned int byte_perm(unsigned int x, unsigned int y, unsigned int s) {
+#if defined(__CUDA_ARCH__)
+    return __byte_perm(x, y, s);
+#else
+    const unsigned long long xy = (static_cast<unsigned long long>(y) << 32) | x;
+    unsigned int r = 0;
+    for (int n = 0; n < 4; ++n) r |= static_cast<unsigned int>((xy >> (8 * ((s >> (4 * n)) & 7u))) & 0xffu) << (8 * n);
+    return r;
+#endif
+}
+
 ASARF_HD ASARF_INLINE int popc_u32(unsigned int v) {
 #if defined(__CUDA_ARCH__)
     return __popc(v);
@@ -288,6 +300,47 @@ ASARF_HD ASARF_INLINE void raw_stats_quad(const RawStatsArgs& a, const RawStatsS
                     }
                 }
             }
+        }
+        // Interior batch: every line and the one before it counted, filled and read through a
+        // whole window.  The group's I and Q bytes are packed into one word each, so every sum
+        // is one byte-lane dot product and nothing is masked per line.
+        bool interior = yg != ys && yg + kStatsBatch <= y1 && pfb == colbits;
+#pragma unroll
+        for (int u = 0; u < kStatsBatch; ++u) interior = interior && vec[u];
+        if (interior) {
+            const unsigned int cm = ncol >= 4 ? 0xffffffffu : (1u << (8 * ncol)) - 1u;
+            unsigned int pI = byte_perm(pI0, pI1, 0x6420u), pQ = byte_perm(pQ0, pQ1, 0x6420u);
+            unsigned int psI = dp4(pI, kOnes, 0u), psQ = dp4(pQ, kOnes, 0u);
+#pragma unroll
+            for (int u = 0; u < kStatsBatch; ++u) {
+                const unsigned int wa = hi_word ? lo[u].y : lo[u].x;
+                const unsigned int wb = hi_word ? hi[u].x : lo[u].y;
+                const unsigned int wc = hi_word ? hi[u].y : hi[u].x;
+                const unsigned int w0u = funnel_r(wa, wb, sh), w1u = funnel_r(wb, wc, sh);
+                const unsigned int I = byte_perm(w0u, w1u, 0x6420u) & cm;
+                const unsigned int Q = byte_perm(w0u, w1u, 0x7531u) & cm;
+                const unsigned int sI = dp4(I, kOnes, 0u), sQ = dp4(Q, kOnes, 0u);
+                si += sI;
+                sq += sQ;
+                sii = dp4(I, I, sii);
+                sqq = dp4(Q, Q, sqq);
+                siq = dp4(I, Q, siq);
+                l1 += psI;
+                l2 += psQ;
+                l3 += sI;
+                l4 += sQ;
+                l5 = dp4(pI, I, l5);
+                l6 = dp4(pQ, Q, l6);
+                l7 = dp4(pI, Q, l7);
+                l8 = dp4(pQ, I, l8);
+                pI = I, pQ = Q, psI = sI, psQ = sQ;
+            }
+            cnt += static_cast<unsigned int>(kStatsBatch * ncol);
+            l0 += static_cast<unsigned int>(kStatsBatch * ncol);
+            // back to the two-word form the general loop carries (I or Q bytes in lanes 0 and 2)
+            pI0 = byte_perm(pI, 0u, 0x4140u), pI1 = byte_perm(pI, 0u, 0x4342u);
+            pQ0 = byte_perm(pQ, 0u, 0x4140u), pQ1 = byte_perm(pQ, 0u, 0x4342u);
+            continue;
         }
 #pragma unroll
         for (int u = 0; u < kStatsBatch; ++u) {
