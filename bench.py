@@ -2,7 +2,7 @@
 """Benchmark of the range-Doppler focusing path on B200.
 
 Metric: raw Msamples/s focused = (range samples x azimuth lines of every scene) / time.
-One step = one full focus of one ERS-like 5616 x 28000 5-bit scene (the BASELINE's
+One step = one full focus of one ERS-like 5616 x 28000 5-bit scene (the headline
 single-GPU configuration): raw I/Q bytes resident in HBM -> IQ statistics + Doppler
 centroid -> range compression -> azimuth FFT / RCMC / matched filter / IFFT -> results
 window -> 5-look multilook + range spreading loss -> slant-to-ground resampling.
