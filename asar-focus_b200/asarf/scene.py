@@ -139,9 +139,8 @@ class Scene:
         return v
 
     # ------------------------------------------------------------------ geometry setup
-    def prepare(self, lib=None) -> "Scene":
-        """Build the orbit, geolocate the scene centre, fix the processing velocity."""
-        lib = lib or _lib.load_library()
+    def build_orbit(self) -> "Scene":
+        """State vectors of the circular 800 km orbit, centred on the scene (pure Python)."""
         rs = R_EARTH + self.altitude
         w = math.sqrt(GM / rs ** 3)
         inc = math.radians(98.5)
@@ -151,7 +150,6 @@ class Scene:
         theta_c = math.radians(30.0)
         # 5 state vectors 10 s apart centred on the scene (more for long strips)
         n_osv = max(5, int(math.ceil(t_scene / 10.0)) + 3)
-        t0 = -t_scene / 2 - 10.0 * ((n_osv - 1) // 2) + t_scene / 2
         t0_us = 1_000_000_000
         self.first_line_time_us = t0_us
         osv = []
@@ -162,14 +160,25 @@ class Scene:
             vel = rs * w * (-math.sin(th) * e1 + math.cos(th) * e2)
             osv.append((t0_us + int(round(t * 1e6)), tuple(pos), tuple(vel)))
         self.osv = osv
-        del t0
+        return self
+
+    def prepare(self, lib=None, geometry=None) -> "Scene":
+        """Build the orbit, geolocate the scene centre, fix the processing velocity.
+
+        ``geometry`` supplies the three FP64 steps (``interpolate_orbit(osv, time_us) ->
+        (pos, vel)``, ``geolocate(vel, pos, guess, slant_range) -> xyz``,
+        ``estimate_vr(scene) -> vr_poly``); by default they are the library's
+        asarf_interpolate_orbit, asarf_geolocate and asarf_estimate_processing_velocity.
+        """
+        if geometry is None:
+            geometry = LibraryGeometry(lib or _lib.load_library())
+        self.build_orbit()
+        osv = self.osv
         # scene centre: right of the ground track at the mid slant range
         tc = self.first_line_time_us + int(self.line_time_interval * (self.azimuth_size // 2) * 1e6)
-        o = _lib.Osv()
-        arr = (_lib.Osv * len(osv))(*[_lib.Osv(t, (C.c_double * 3)(*p), (C.c_double * 3)(*v)) for t, p, v in osv])
-        _lib.check(lib, lib.asarf_interpolate_orbit(arr, len(osv), tc, C.byref(o)), "interpolate_orbit")
-        pos = np.array(o.pos[:])
-        vel = np.array(o.vel[:])
+        pos, vel = geometry.interpolate_orbit(osv, tc)
+        pos = np.asarray(pos, dtype=np.float64)
+        vel = np.asarray(vel, dtype=np.float64)
         up = pos / np.linalg.norm(pos)
         right = np.cross(vel / np.linalg.norm(vel), up)
         nk = self.range_size - self.chirp_samples
@@ -177,19 +186,13 @@ class Scene:
         ground = math.sqrt(max(r_mid ** 2 - self.altitude ** 2, 1.0))
         guess = (up + (ground / R_EARTH) * right)
         guess = guess / np.linalg.norm(guess) * R_EARTH
-        out = (C.c_double * 3)()
-        _lib.check(lib, lib.asarf_geolocate((C.c_double * 3)(*vel), (C.c_double * 3)(*pos),
-                                            (C.c_double * 3)(*guess), r_mid, out), "geolocate")
-        self.center_point = tuple(out[:])
+        self.center_point = tuple(float(v) for v in geometry.geolocate(vel, pos, guess, r_mid))
         vp = float(np.linalg.norm(osv[len(osv) // 2][2]))
         self.vr_poly_init = (0.0, 0.0, math.sqrt(0.88 * vp * vp))
         if self.vr_given is not None:
             self.vr_poly = (0.0, 0.0, float(self.vr_given))
         else:
-            sc = self.to_c(estimate=True)
-            vr = (C.c_double * 3)()
-            _lib.check(lib, lib.asarf_estimate_processing_velocity(C.byref(sc[0]), vr), "estimate_vr")
-            self.vr_poly = tuple(vr[:])
+            self.vr_poly = tuple(float(v) for v in geometry.estimate_vr(self))
         return self
 
     # ------------------------------------------------------------------ exports
@@ -252,6 +255,32 @@ class Scene:
             raw_format=self.raw_format, raw_line_bytes=self.raw_line_bytes,
             fbaq_tables=self.fbaq_tables,
         )
+
+
+class LibraryGeometry:
+    """The FP64 geometry steps of Scene.prepare through the library's C ABI."""
+
+    def __init__(self, lib):
+        self.lib = lib
+
+    def interpolate_orbit(self, osv, time_us):
+        arr = (_lib.Osv * len(osv))(*[_lib.Osv(t, (C.c_double * 3)(*p), (C.c_double * 3)(*v)) for t, p, v in osv])
+        o = _lib.Osv()
+        _lib.check(self.lib, self.lib.asarf_interpolate_orbit(arr, len(osv), int(time_us), C.byref(o)),
+                   "interpolate_orbit")
+        return tuple(o.pos[:]), tuple(o.vel[:])
+
+    def geolocate(self, vel, pos, guess, slant_range):
+        out = (C.c_double * 3)()
+        _lib.check(self.lib, self.lib.asarf_geolocate((C.c_double * 3)(*vel), (C.c_double * 3)(*pos),
+                                                      (C.c_double * 3)(*guess), float(slant_range), out), "geolocate")
+        return tuple(out[:])
+
+    def estimate_vr(self, scene):
+        sc = scene.to_c(estimate=True)
+        vr = (C.c_double * 3)()
+        _lib.check(self.lib, self.lib.asarf_estimate_processing_velocity(C.byref(sc[0]), vr), "estimate_vr")
+        return tuple(vr[:])
 
 
 # ---------------------------------------------------------------------- the workloads

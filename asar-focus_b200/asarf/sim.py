@@ -42,6 +42,76 @@ def target_grid(sc: Scene) -> list[tuple[float, float]]:
     return [(float(round(x)) + 0.0, float(round(y)) + 0.0) for y in ys for x in xs]
 
 
+def _orbit_state(sc: Scene, time_us: int):
+    """Position and velocity of the scene's circular orbit at an absolute time (analytic,
+    the curve the state vectors of Scene.build_orbit sample)."""
+    from .scene import GM, R_EARTH
+    rs = R_EARTH + sc.altitude
+    w = math.sqrt(GM / rs ** 3)
+    inc = math.radians(98.5)
+    e1 = np.array([1.0, 0.0, 0.0])
+    e2 = np.array([0.0, math.cos(inc), math.sin(inc)])
+    t_scene = sc.azimuth_size / sc.prf
+    t = (time_us - sc.first_line_time_us) * 1e-6
+    th = math.radians(30.0) + w * (t - t_scene / 2)
+    return rs * (math.cos(th) * e1 + math.sin(th) * e2), rs * w * (-math.sin(th) * e1 + math.cos(th) * e2)
+
+
+def truth_vr_poly(sc: Scene) -> tuple:
+    """Effective velocity of the simulated world, quadratic in range pixel (highest power first).
+
+    It is the hyperbolic range-history coefficient of a point on the WGS84 ellipsoid seen from
+    the analytic orbit, fitted over 9 positions across the synthetic aperture at 10 range
+    positions, so that a processor that estimates Vr from the state vectors recovers it.  It
+    depends only on the scene description, not on any processor's estimate, so every
+    process simulating a scene produces the same raw bytes.
+    """
+    if sc.vr_given is not None:
+        return (0.0, 0.0, float(sc.vr_given))
+    if not sc.osv:
+        sc.build_orbit()
+    a_e, b_e = 6378137.0, 6356752.314245
+    lti = 1.0 / sc.prf
+    mid = sc.azimuth_size // 2
+    tc = sc.first_line_time_us + (int(lti * mid * 1e6) & 0xFFFFFFFF)
+    pc, vc = _orbit_state(sc, tc)
+    up = pc / np.linalg.norm(pc)
+    right = np.cross(vc / np.linalg.norm(vc), up)
+    nk = sc.range_size - sc.chirp_samples
+    step = nk // 10
+    vr_init = math.sqrt(0.88) * float(np.linalg.norm(vc))
+    xs, vs = [], []
+    for x in range(0, nk, step):
+        r0 = sc.slant_range_first + x * sc.range_spacing
+        ground = math.sqrt(max(r0 ** 2 - sc.altitude ** 2, 1.0))
+        t = up + (ground / a_e) * right
+        t = t / np.linalg.norm(t) * a_e
+        for _ in range(60):  # zero Doppler, slant range r0, on the ellipsoid
+            d = t - pc
+            f = np.array([vc @ d, d @ d - r0 * r0, (t[0] / a_e) ** 2 + (t[1] / a_e) ** 2 + (t[2] / b_e) ** 2 - 1])
+            jac = np.array([vc, 2 * d, [2 * t[0] / a_e ** 2, 2 * t[1] / a_e ** 2, 2 * t[2] / b_e ** 2]])
+            dt = np.linalg.solve(jac, -f)
+            t = t + dt
+            if np.linalg.norm(dt) < 1e-6:
+                break
+        ka = 2 * vr_init * vr_init / (sc.wavelength * r0)
+        ap = int(math.floor((sc.prf * sc.az_bw_frac / 2) / ka * sc.prf + 0.5))
+        hs = int(ap / 8)
+        ts, ys = [], []
+        for i in range(9):
+            idx = mid + (i - 4) * hs
+            ti = sc.first_line_time_us + (int(lti * idx * 1e6) & 0xFFFFFFFF)
+            p, _ = _orbit_state(sc, ti)
+            dd = p - t
+            ys.append(dd @ dd - r0 * r0)
+            ts.append((tc - ti) * 1e-6)
+        ts = np.asarray(ts)
+        coef = np.linalg.lstsq(np.stack([np.ones(9), ts * ts], axis=1), np.asarray(ys), rcond=None)[0]
+        xs.append(x)
+        vs.append(math.sqrt(coef[1]))
+    return tuple(float(c) for c in np.polyfit(np.asarray(xs, float), np.asarray(vs), 2))
+
+
 def simulate(sc: Scene, device: str | torch.device = "cpu", noise_rel: float = 0.25,
              return_field: bool = False):
     """Return (raw uint8 numpy [Na, 2*spl], truth dict)."""
@@ -53,7 +123,7 @@ def simulate(sc: Scene, device: str | torch.device = "cpu", noise_rel: float = 0
     prf = sc.prf
     lam = sc.wavelength
     dr = sc.range_spacing
-    vr_poly = sc.vr_poly if sc.vr_poly is not None else (0.0, 0.0, 7100.0)
+    vr_poly = truth_vr_poly(sc)
     gen = torch.Generator(device=dev)
     gen.manual_seed(int(sc.seed))
     cdt = torch.complex64

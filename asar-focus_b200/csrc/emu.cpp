@@ -7,6 +7,7 @@
 #include <cstring>
 #include <vector>
 
+#include "context_cache.h"
 #include "asarf.h"
 #include "backend.h"
 #include "bodies.cuh"
@@ -266,6 +267,25 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
     d_out->applied_cos = s.cos_c;
     d_out->errors = s.errors;
     return ASARF_OK;
+}
+
+// Test hook of the host emulation only: drives the context-keyed address cache of the
+// allocation-free entry point (context_cache.h) with made-up context ids and a resolver that
+// hands out a fresh fake address on every call.  For each key i, addrs[i] receives the
+// address returned and the function returns how many times the resolver ran.
+extern "C" int asarf_emu_context_cache_probe(const unsigned long long* ids, int n, unsigned long long* addrs) {
+    static asarf::ContextAddressCache<4> cache;
+    static unsigned long long next_fake = 0x1000;
+    int resolutions = 0;
+    for (int i = 0; i < n; ++i) {
+        void* p = nullptr;
+        bool resolved = false;
+        cache.get(ids[i], [](void** q) { *q = reinterpret_cast<void*>(next_fake); next_fake += 0x1000; return 0; },
+                  &p, &resolved);
+        resolutions += resolved ? 1 : 0;
+        addrs[i] = reinterpret_cast<unsigned long long>(p);
+    }
+    return resolutions;
 }
 
 namespace asarf {

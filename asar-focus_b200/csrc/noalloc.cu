@@ -13,6 +13,8 @@
 // loaded, on every GPU that loads it.  All calls on a device share it, so calls whose
 // kernels overlap on the GPU (two streams, two host threads) race and corrupt each
 // other's sums; serialise them.  Each call clears the accumulators before use.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -22,6 +24,7 @@
 #include "asarf.h"
 #include "backend.h"
 #include "bodies.cuh"
+#include "context_cache.h"
 
 namespace asarf {
 namespace {
@@ -36,26 +39,67 @@ static_assert(sizeof(NoallocScratch) <= kNoallocScratchBytes, "scratch layout ex
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
+ContextAddressCache<64> g_scratch_cache;
 
-// Device address of the scratch array on the current device, resolved once per device.
-// In host code the array's name is only a stand-in symbol, never a usable pointer.
+// Unique id of the calling thread's current CUDA context (0 when none is current yet),
+// through the driver entry points the runtime exposes.
+int current_context_id(unsigned long long* id) {
+    static std::once_flag once;
+    static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id)
+        return set_error(ASARF_ERR_CUDA, "raw_statistics_noalloc: cuCtxGetCurrent / cuCtxGetId unavailable");
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS)
+        return set_error(ASARF_ERR_CUDA, "raw_statistics_noalloc: cuCtxGetCurrent failed");
+    *id = 0;
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS)
+        return set_error(ASARF_ERR_CUDA, "raw_statistics_noalloc: cuCtxGetId failed");
+    return ASARF_OK;
+}
+
+int resolve_scratch(void** p) {
+    *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(p, g_noalloc_scratch);
+    if (e != cudaSuccess || !*p)
+        return set_error(ASARF_ERR_CUDA, "raw_statistics_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    return ASARF_OK;
+}
+
+// Device address of the scratch array in the current CUDA context, resolved once per
+// context (a new context after cudaDeviceReset, or a host application's own context, gets
+// its own lookup).  In host code the array's name is only a stand-in symbol, never a usable
+// pointer.  With no context current yet, the lookup itself makes the runtime bind the
+// device's primary context, whose id then keys the entry.
 int scratch_address(NoallocScratch** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return set_error(ASARF_ERR_CUDA, "raw_statistics_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return set_error(ASARF_ERR_INVALID, "raw_statistics_noalloc: device %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return set_error(ASARF_ERR_CUDA, "raw_statistics_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-        g_scratch_addr[dev] = p;
+    unsigned long long id = 0;
+    int rc = current_context_id(&id);
+    if (rc) return rc;
+    void* p = nullptr;
+    if (id == 0) {
+        rc = resolve_scratch(&p);
+        if (rc) return rc;
+        rc = current_context_id(&id);
+        if (rc) return rc;
+        if (id == 0) return set_error(ASARF_ERR_CUDA, "raw_statistics_noalloc: no CUDA context after set-up");
+        rc = g_scratch_cache.get(id, [p](void** q) { *q = p; return 0; }, &p);
+    } else {
+        rc = g_scratch_cache.get(id, resolve_scratch, &p);
     }
-    *out = static_cast<NoallocScratch*>(g_scratch_addr[dev]);
+    if (rc) return rc;
+    *out = static_cast<NoallocScratch*>(p);
     return ASARF_OK;
 }
 

@@ -245,18 +245,20 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     sampler.start()
     time.sleep(0.25)
     plan.enable_timing(args.steps)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    # one event between consecutive steps: the mean over the K steps is the headline, the
+    # median of the per-step times is reported beside it (the reference arm reports both too)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     torch.cuda.synchronize()
     _barrier(world)
-    e0.record(stream)
-    for _ in range(args.steps):
+    ev[0].record(stream)
+    for i in range(args.steps):
         plan.focus(raw_d, out_d, stream=st)
-    e1.record(stream)
+        ev[i + 1].record(stream)
     torch.cuda.synchronize()
     _barrier(world)
     clocks = sampler.stop()
-    ms_step = e0.elapsed_time(e1) / args.steps
+    ms_step = ev[0].elapsed_time(ev[-1]) / args.steps
+    ms_median = statistics.median(ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps))
     ktimes, kruns = plan.kernel_times()
     ms_max = _max_over_ranks(ms_step, world)
     samples = sc.range_size * sc.azimuth_size
@@ -320,10 +322,12 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         return
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "ms_statistic": "mean of steps",
+        "ms_median": round(ms_median, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32 (complex64 data, FP64 geometry)", "data": "synthetic",
         "config": {"workload": f"{args.workload}: {_describe(sc)}",
                    "range_samples": sc.range_size, "azimuth_lines": sc.azimuth_size, "scenes_per_step": world,
+                   "raw_sha256": _sha256(raw_np), "vr_poly": list(sc.vr_poly),
                    "l2": f"inputs larger than L2 (raw {raw_np.nbytes / 1e6:.0f} MB, complex images "
                          f"{dims['az_pad'] * dims['nk'] * 8 / 1e9:.2f} GB each)",
                    "parallelism": f"replicas x{world} (independent scenes)",
@@ -343,6 +347,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                               "frac": round(pipe / (ms_max * 1e-3) / 1e9 / peak, 4), "unit": "GB/s"},
         "kernel_ms_per_step": {k: round(v, 4) for k, v in per_launch.items()},
         "gpu_launches": 7 * args.steps,
+        "native_libs_mapped": _mapped_native_libs(),
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -350,21 +355,62 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+class OracleGeometry:
+    """The scene set-up's FP64 geometry through the oracle's restatement (oracle/geometry.py),
+    so that the reference arm's process never loads libasarf.so."""
+
+    def __init__(self):
+        from oracle import geometry as geo
+        self.geo = geo
+
+    def interpolate_orbit(self, osv, time_us):
+        o = self.geo.interpolate_orbit([self.geo.Osv(*v) for v in osv], int(time_us))
+        return o.pos, o.vel
+
+    def geolocate(self, vel, pos, guess, slant_range):
+        return self.geo.geolocate(vel, pos, guess, slant_range)
+
+    def estimate_vr(self, sc):
+        return self.geo.estimate_processing_velocity(
+            [self.geo.Osv(*v) for v in sc.osv], sc.first_line_time_us, sc.line_time_interval, sc.center_point,
+            sc.slant_range_first, sc.range_spacing, sc.carrier_frequency, sc.vr_poly_init, sc.prf, sc.az_bw_frac,
+            sc.range_size, sc.chirp_samples, sc.azimuth_size)
+
+
+def _mapped_native_libs() -> list[str]:
+    """Shared objects of this repository mapped into the current process."""
+    out = set()
+    try:
+        for line in open("/proc/self/maps"):
+            path = line.split()[-1] if len(line.split()) >= 6 else ""
+            if path.endswith(".so") and path.startswith(str(ROOT)):
+                out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def _sha256(raw) -> str:
+    import hashlib
+    return hashlib.sha256(memoryview(raw).cast("B")).hexdigest()
+
+
 def run_reference(args, rank: int, world: int) -> None:
+    """The reference's own CUDA build (oracle/_ref/libasar_ref.so) on the same seeded scene.
+    Nothing of the product is loaded here: the scene geometry (orbit interpolation,
+    geolocation, processing-velocity fit) comes from the oracle's FP64 restatement."""
     if rank != 0:
         return
     import numpy as np
     import torch
-    import asarf
     from asarf import sim
     from oracle import ref_lib
 
     if not ref_lib.available():
         print(json.dumps({"impl": "reference", "unavailable": f"reference build missing ({ref_lib.REF_LIB})"}))
         return
-    lib = asarf.load_library()
     sc = make_scene(args.workload, 1001)
-    sc.prepare(lib)
+    sc.prepare(geometry=OracleGeometry())
     raw_np, _ = sim.simulate(sc, device="cuda")
     raw_d = torch.from_numpy(raw_np).cuda()
     scc, keep = sc.to_c()
@@ -385,28 +431,29 @@ def run_reference(args, rank: int, world: int) -> None:
         e2e.append(r["ms_wall"])
     clocks = sampler.stop()
     samples = sc.range_size * sc.azimuth_size
-    # median per step: the reference allocates and synchronises inside every call, so a single
-    # host-side stall (e.g. a page-mapping of a fresh allocation) would skew a mean of a few steps
-    # against it; the median is the generous reading for the reference
-    ms = statistics.median(dev_ms)
+    # mean over the timed steps, as the optimised arm reports; the median beside it
+    ms = statistics.fmean(dev_ms)
     value = samples / ms / 1e3
-    e2e_ms = statistics.median(e2e)
+    e2e_ms = statistics.fmean(e2e)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "ms_statistic": "median of steps",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "ms_statistic": "mean of steps",
+        "ms_median": round(statistics.median(dev_ms), 3),
         "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (cuFFT)", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: ERS-like {sc.range_size} range x {sc.azimuth_size} azimuth "
-                               f"(same seeded scene as the optimised arm)",
+        "config": {"workload": f"{args.workload}: {_describe(sc)}",
                    "range_samples": sc.range_size, "azimuth_lines": sc.azimuth_size,
+                   "raw_sha256": _sha256(raw_np), "vr_poly": list(sc.vr_poly),
                    "l2": "inputs larger than L2", "parallelism": "single GPU"},
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": "the reference's own CUDA build (asar-focus sar/ + cuda_util/, cuFFT) on this "
                                    "B200, driven by one host thread; the reference has no CPU implementation"},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "host_api_value": round(samples / e2e_ms / 1e3, 1),
-                "host_api_note": "wall clock through ConvertErsImSamplesToComplex (host raw) to host output"},
+                "host_api_note": "wall clock through ConvertErsImSamplesToComplex (host raw) to host output, "
+                                 "mean of steps"},
         "device_ms_steps": [round(v, 2) for v in dev_ms],
+        "native_libs_mapped": _mapped_native_libs(),
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)

@@ -218,12 +218,15 @@ typedef struct asarf_raw_stats {
  * estimate of CalculateDopplerCentroid) and writes them to `d_out`, a device buffer the
  * caller owns.  Its only scratch is a fixed 8 KiB array in this library's static device
  * memory, held on every GPU that loads the library until exit; it bounds the number of
- * Doppler blocks to 80 (any range_size >= 32 gives 32 or 33) and larger counts are
- * rejected with ASARF_ERR_INVALID.  All calls on a device share that array: calls whose
- * work overlaps on the GPU race, so issue them in order on one stream.  The first call on
- * each device looks up the array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  `stats_stride` is the padded width the reference runs
- * its gain / phase sums over (its range FFT size; 0 = data samples only). */
+ * Doppler blocks to 80 and larger counts are rejected with ASARF_ERR_INVALID (blocks are
+ * floor(range_size / 32) samples wide, so range_size 32..63 gives range_size blocks, at most
+ * 63, and every larger size gives 32 to 63: the bound is never reached).  All calls on a
+ * device share that array: calls whose work overlaps on the GPU race, so issue them in order
+ * on one stream.  The first call in each CUDA context looks up the array's device address
+ * (cudaGetSymbolAddress), keyed by the context's id: after cudaDeviceReset, or under a host
+ * application's own driver context, the next call looks it up again.  Make that first call
+ * in a context before any stream capture.  `stats_stride` is the padded width the reference
+ * runs its gain / phase sums over (its range FFT size; 0 = data samples only). */
 int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_line_bytes, int32_t samples_per_line,
                                  int32_t range_size, int32_t azimuth_size, const uint16_t* d_swst, int32_t min_swst,
                                  int64_t total_raw_samples, int32_t stats_stride, double prf, asarf_raw_stats* d_out,

@@ -16,6 +16,7 @@ float32 operation sequence.
 Parity pinning: the reference ships no golden vectors or known-answer tests for
 this path (its unit tests cover only parsing helpers).  The oracle is pinned
 against the reference's own CUDA build (``oracle/ref_build``: the reference's
-``sar/`` + ``cuda_util/`` sources compiled for sm_100a, run on a B200), see
-``tests/test_ref_pin.py``.
+``sar/`` + ``cuda_util/`` sources compiled for sm_100a, run on a B200): the stored
+reference outputs in ``tests/golden`` are checked on the CPU by ``tests/test_golden.py``,
+and the reference build runs beside the oracle on the GPU in ``tests/test_gpu_parity.py``.
 """
