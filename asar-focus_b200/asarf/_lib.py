@@ -37,8 +37,12 @@ RAW_ASAR_FBAQ4 = 1
 class Options(C.Structure):
     _fields_ = [("rc_fft_len", C.c_int32), ("ref_compat_stats", C.c_int32), ("iq_padding_ref", C.c_int32),
                 ("dc_poly_given", C.c_int32), ("dc_poly", C.c_double * 3), ("product", C.c_int32),
-                ("record_header_bytes", C.c_int32), ("calibration", C.c_float), ("sq_stats", C.c_int32)]
+                ("record_header_bytes", C.c_int32), ("calibration", C.c_float), ("sq_stats", C.c_int32),
+                ("precision", C.c_int32)]
 
+
+PRECISION_FP32 = 0
+PRECISION_SPLIT = 1
 
 PRODUCT_DETECTED = 0
 PRODUCT_IMP_MDS = 1
@@ -51,7 +55,7 @@ class Dims(C.Structure):
         ("n1", C.c_int32), ("n2", C.c_int32), ("slc_cols", C.c_int32), ("out_rows", C.c_int32 * 2),
         ("out_cols", C.c_int32 * 2), ("out_rows_max", C.c_int32), ("out_cols_max", C.c_int32),
         ("max_aperture", C.c_int32), ("vr_poly", C.c_double * 3), ("device_bytes", C.c_size_t),
-        ("out_bytes_max", C.c_int64),
+        ("out_bytes_max", C.c_int64), ("precision", C.c_int32), ("split_radix", C.c_int32), ("split_m", C.c_int32),
     ]
 
 

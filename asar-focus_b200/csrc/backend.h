@@ -24,6 +24,9 @@ int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh
 int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream);
 int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, unsigned int* err,
                   void* stream);
+// split-precision range-Doppler block (tensor-core forward transform); device build only
+int backend_az_rd_split(const AzRdArgs& a, const AzRdSplit& sp, const void* tmap, int tiles, int nblocks,
+                        LaunchShape sh, unsigned int* err, void* stream);
 int backend_tail(const TailArgs& a, int rows, LaunchShape sh, unsigned int* err, void* stream);
 int backend_condition(const ConditionArgs& a, int rows, void* stream);
 int backend_product_stats(const ProductStatsArgs& a, void* stream);  // partials then fold

@@ -1108,6 +1108,9 @@ struct AzRdOut {
     }
 };
 
+// FWD = false: the caller has already put the tile through the forward transform (the
+// split-precision kernel's tensor-core DFT) and synchronised.
+template <bool FWD = true>
 ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s,
                                       const ColParams* cps, const int* fbin, unsigned int* err_flag, bool preloaded) {
     const int x0 = tile * a.xt;
@@ -1122,8 +1125,10 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
             s[t] = v;
         }
     }
-    ASARF_SYNC();
-    fft_forward_pairs(a.plan2, s, wt, wt, tid, nthr);
+    if constexpr (FWD) {
+        ASARF_SYNC();
+        fft_forward_pairs(a.plan2, s, wt, wt, tid, nthr);
+    }
     // RCMC + matched filter.  Every output (row p, column c) reads taps of row p only, so a
     // row is computed into registers by one warp (lane = column, xt <= 64), the warp
     // synchronises, and writes it back in place: no block-wide barrier per row.

@@ -289,6 +289,9 @@ extern "C" int asarf_emu_context_cache_probe(const unsigned long long* ids, int 
 }
 
 namespace asarf {
+int backend_az_rd_split(const AzRdArgs&, const AzRdSplit&, const void*, int, int, LaunchShape, unsigned int*, void*) {
+    return set_error(ASARF_ERR_INVALID, "split precision runs on the tensor cores only (no host emulation)");
+}
 int event_sync(void*) { return ASARF_OK; }
 void* stream_create() { return std::calloc(1, 8); }
 void stream_destroy(void* s) { std::free(s); }

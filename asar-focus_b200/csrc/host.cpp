@@ -285,6 +285,57 @@ bool smooth(int n) {
     return n == 1;
 }
 
+// bf16 of a float, round to nearest even (finite inputs).
+static uint16_t bf16_rn(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return static_cast<uint16_t>(u >> 16);
+}
+static float bf16_to_float(uint16_t h) {
+    const uint32_t u = static_cast<uint32_t>(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// Tables of the split-precision forward transform of length n = R * m: the m-point DFT matrix
+// as the B operand (rows = output (slot, re / im), K = input (mm, re / im)) in the canonical
+// no-swizzle K-major layout, bf16 hi image then lo image; and the twiddles W_n^(r k1(s)),
+// [r][s].  Output slot s holds frequency k1(s) = drev[R s] (the FP32 transform's order).
+// FP64 throughout, rounded once.
+void split_dft_tables(int n, int R, const std::vector<int>& drev, std::vector<unsigned char>& img,
+                      std::vector<float2>& tw) {
+    const int m = n / R;
+    img.assign(2 * static_cast<size_t>(kSplitMatrixBytes), 0);
+    auto put = [&](int row, int k, double v) {
+        const float f = static_cast<float>(v);
+        const uint16_t hi = bf16_rn(f);
+        const uint16_t lo = bf16_rn(f - bf16_to_float(hi));
+        const uint32_t off = umma_offset(row, k, kSplitK);
+        std::memcpy(&img[off], &hi, 2);
+        std::memcpy(&img[kSplitMatrixBytes + off], &lo, 2);
+    };
+    for (int sl = 0; sl < m; ++sl) {
+        const int k1 = drev[static_cast<size_t>(R) * sl];
+        for (int j = 0; j < m; ++j) {
+            const double a = -2.0 * kPi * static_cast<double>((static_cast<long long>(j) * k1) % m) / m;
+            const double fr = std::cos(a), fi = std::sin(a);
+            put(2 * sl, 2 * j, fr);
+            put(2 * sl, 2 * j + 1, -fi);
+            put(2 * sl + 1, 2 * j, fi);
+            put(2 * sl + 1, 2 * j + 1, fr);
+        }
+    }
+    tw.assign(static_cast<size_t>(R) * m, make_float2(1.0f, 0.0f));
+    for (int r = 0; r < R; ++r)
+        for (int sl = 0; sl < m; ++sl) {
+            const int k1 = drev[static_cast<size_t>(R) * sl];
+            const double a = -2.0 * kPi * static_cast<double>((static_cast<long long>(r) * k1) % n) / n;
+            tw[static_cast<size_t>(r) * m + sl] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+        }
+}
+
 void matched_filter_table(const std::complex<float>* chirp, int nc, const HostFft& fft, std::vector<float2>& mf) {
     // conj(DFT_L(replica)) / L in FP64, stored in the forward transform's digit-reversed order
     const int L = fft.plan.n;
@@ -407,6 +458,7 @@ void asarf_default_options(asarf_options* opt) {
     opt->record_header_bytes = 17;  // main.cc: 12 + 1 + 4
     opt->calibration = 1.0f;
     opt->sq_stats = 0;
+    opt->precision = ASARF_PRECISION_FP32;
 }
 
 int32_t asarf_fft_size_above(int32_t v) { return fft_size_above(v); }
@@ -549,7 +601,15 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     const int n_ctr = ct_radices(p->rc_len, ctr);
     const bool rc_ok = n_ctr ? build_fft_radices(p->rc_len, std::vector<int>(ctr, ctr + n_ctr), p->rc)
                              : build_fft(p->rc_len, p->rc);
-    if (!rc_ok || !build_fft_radices(p->n1, strided_radices(p->n1), p->f1) || !build_fft(p->n2, p->f2) || !build_fft(p->az_pad, p->fN)) {
+    // the split-precision form takes the contiguous transform's last radix as its FP32 pass, so
+    // that pass gets the largest radix (smallest tensor-core DFT)
+    std::vector<int> f2_radices = factorize(p->n2);
+    if (opt.precision == ASARF_PRECISION_SPLIT && !f2_radices.empty()) {
+        auto big = std::max_element(f2_radices.begin(), f2_radices.end());
+        std::rotate(big, big + 1, f2_radices.end());
+    }
+    if (!rc_ok || !build_fft_radices(p->n1, strided_radices(p->n1), p->f1) ||
+        !build_fft_radices(p->n2, f2_radices, p->f2) || !build_fft(p->az_pad, p->fN)) {
         delete p;
         return set_error(ASARF_ERR_INVALID, "FFT schedule failed");
     }
@@ -927,6 +987,39 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         d.n2_box = n2_box;
     }
 
+    // ---- split precision: n2 = R * m with R the FP32 plan's last radix (so that its digit
+    // reversal puts frequency k1 + m k2 at position R s + k2) and m <= 32
+    if (opt.precision == ASARF_PRECISION_SPLIT) {
+        const int R = p->f2.plan.radix[p->f2.plan.nst - 1];
+        const int m = p->n2 / R;
+        const bool radix_ok = R == 2 || R == 3 || R == 4 || R == 5 || R == 7 || R == 8;
+        const size_t smem_split = 2 * static_cast<size_t>(kSplitOperandBytes) + 2 * kSplitMatrixBytes + p->sh_rd.smem;
+        if (p->use_tma && radix_ok && m >= 2 && 2 * m <= kSplitK && d.wt <= kSplitRows &&
+            smem_split <= smem_optin_limit()) {
+            std::vector<unsigned char> img;
+            std::vector<float2> tws;
+            split_dft_tables(p->n2, R, p->f2.drev, img, tws);
+            unsigned char* bmat = p->alloc<unsigned char>(img.size());
+            float2* tw_dev = p->alloc<float2>(tws.size());
+            if (!bmat || !tw_dev) {
+                delete p;
+                return set_error(ASARF_ERR_CUDA, "device allocation failed (split tables)");
+            }
+            rc = mem_h2d(bmat, img.data(), img.size(), nullptr);
+            rc |= mem_h2d(tw_dev, tws.data(), sizeof(float2) * tws.size(), nullptr);
+            if (rc) {
+                delete p;
+                return set_error(ASARF_ERR_CUDA, "split table upload failed");
+            }
+            p->split = true;
+            p->a_split.bmat = bmat;
+            p->a_split.tw = tw_dev;
+            p->a_split.radix = R;
+            p->a_split.m = m;
+            p->sh_rd_split = {512, smem_split};
+        }
+    }
+
     const size_t lim = smem_optin_limit();
     if (p->sh_rc.smem > lim || p->sh_st.smem > lim || p->sh_rd.smem > lim || p->sh_tail.smem > lim) {
         const size_t a1 = p->sh_rc.smem, a2 = p->sh_st.smem, a3 = p->sh_rd.smem;
@@ -953,6 +1046,9 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     dm.max_aperture = max_ap;
     for (int k = 0; k < 3; ++k) dm.vr_poly[k] = p->vr_poly[k];
     dm.device_bytes = p->bytes;
+    dm.precision = p->split ? ASARF_PRECISION_SPLIT : ASARF_PRECISION_FP32;
+    dm.split_radix = p->split ? p->a_split.radix : 0;
+    dm.split_m = p->split ? p->a_split.m : 0;
     *out = p;
     return ASARF_OK;
 }
@@ -1017,8 +1113,10 @@ int asarf_focus(asarf_plan* p, const uint8_t* d_raw, const uint16_t* d_swst, int
     rc = backend_az_strided(p->a_fwd, p->use_tma ? p->tmapA3 : nullptr, p->tiles1, p->n2, p->sh_st, stream);
     if (rc) return rc;
     mark();
-    rc = backend_az_rd(p->a_rd, p->use_tma ? p->tmapA2 : nullptr, p->tiles2, p->n1, p->sh_rd, &p->state->errors,
-                       stream);
+    rc = p->split ? backend_az_rd_split(p->a_rd, p->a_split, p->tmapA2, p->tiles2, p->n1, p->sh_rd_split,
+                                        &p->state->errors, stream)
+                  : backend_az_rd(p->a_rd, p->use_tma ? p->tmapA2 : nullptr, p->tiles2, p->n1, p->sh_rd,
+                                  &p->state->errors, stream);
     if (rc) return rc;
     mark();
     rc = backend_az_strided(p->a_inv, p->use_tma ? p->tmapB3 : nullptr, p->tiles1, p->n2, p->sh_st, stream);

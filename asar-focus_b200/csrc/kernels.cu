@@ -13,6 +13,7 @@
 #include "asarf.h"
 #include "backend.h"
 #include "bodies.cuh"
+#include "tc.cuh"
 #include "tma.cuh"
 
 namespace asarf {
@@ -176,6 +177,133 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
     az_rd_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, a.use_tma != 0);
 }
 
+// ----------------------------------------------------------------------------- split precision
+// Forward transform of the range-Doppler tile on the tensor cores.  Tile s[l][c], l < n2 =
+// R * m, c < wt <= 128.  For each r < R the sub-sequence x[r + R mm] (mm < m) of every column
+// becomes the bf16 hi + lo operand A (row = column c, K = (mm, re / im)), which multiplies the
+// m-point DFT matrix B (hi + lo, output slot s = frequency k1(s)) as Ahi Bhi + Ahi Blo + Alo Bhi
+// with FP32 accumulation in TMEM; the result times W_n2^(r k1(s)) goes back to row r + R s
+// (a row of the same sub-sequence, already consumed).  A radix-R FP32 pass over rows
+// R s .. R s + R - 1 then leaves frequency k1(s) + m k2 at row R s + k2: the digit-reversed
+// order of the FP32 forward transform (k1(s) is read from that transform's order table).
+// Returns false (error bit set, products drained) if a product did not complete in time.
+__device__ bool split_forward(const AzRdArgs& a, const AzRdSplit& sp, float2* s, unsigned char* a_hi_p,
+                              unsigned char* a_lo_p, const unsigned char* b_hi_p, const unsigned char* b_lo_p,
+                              uint32_t tmem, uint64_t* mbar, uint32_t& phase, unsigned int* err) {
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int wt = a.wt, R = sp.radix, m = sp.m;
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr uint32_t kIdesc = umma_idesc_bf16(kSplitRows, kSplitN);
+    constexpr uint32_t kSbo = kSplitK * 16;  // 8 rows x K bf16
+    const uint32_t a_hi = smem_u32(a_hi_p), a_lo = smem_u32(a_lo_p);
+    const uint32_t b_hi = smem_u32(b_hi_p), b_lo = smem_u32(b_lo_p);
+    for (int r = 0; r < R; ++r) {
+        // operands: item = (column c, chunk kc of 4 complex inputs = 8 bf16 = 16 bytes)
+        for (int t = tid; t < kSplitRows * (kSplitK / 8); t += nthr) {
+            const int c = t & (kSplitRows - 1), kc = t >> 7;
+            uint32_t hi[4], lo[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int mm = 4 * kc + j;
+                float2 v = make_float2(0.0f, 0.0f);
+                if (c < wt && mm < m) v = s[(r + R * mm) * wt + c];
+                split_bf16x2(v.x, v.y, hi[j], lo[j]);
+            }
+            const uint32_t off = umma_offset(c, 8 * kc, kSplitK);
+            *reinterpret_cast<uint4*>(a_hi_p + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4*>(a_lo_p + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        }
+        fence_async_smem();
+        tc_fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after_sync();
+#pragma unroll
+            for (int ks = 0; ks < kSplitK / 16; ++ks) {
+                const uint32_t o = 256u * ks;  // two 128-byte core-matrix columns per k-step
+                const uint64_t dah = umma_smem_desc(a_hi + o, 128, kSbo), dal = umma_smem_desc(a_lo + o, 128, kSbo);
+                const uint64_t dbh = umma_smem_desc(b_hi + o, 128, kSbo), dbl = umma_smem_desc(b_lo + o, 128, kSbo);
+                umma_bf16(tmem, dah, dbh, kIdesc, ks > 0);
+                umma_bf16(tmem, dah, dbl, kIdesc, true);
+                umma_bf16(tmem, dal, dbh, kIdesc, true);
+            }
+            umma_commit(mbar);
+        }
+        const bool done = mbar_wait(mbar, phase, nullptr);
+        if (__syncthreads_or(!done)) {
+            if (tid == 0) atomicOr(err, kErrMmaTimeout);
+            mbar_wait(mbar, phase, nullptr);  // give the products in flight one more bounded wait
+            return false;
+        }
+        phase ^= 1u;
+        tc_fence_after_sync();
+        // accumulator rows: warp -> TMEM lanes 32 (w % 4) .., columns 16 (w / 4) .. (8 slots)
+        if (warp < 16) {
+            const int q = warp & 3, jb = warp >> 2;
+            float v[16];
+            tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + 16u * jb, v);
+            const int c = 32 * q + lane;
+            if (c < wt) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int slot = 8 * jb + i;
+                    if (slot < m)
+                        s[(r + R * slot) * wt + c] = cmul(make_float2(v[2 * i], v[2 * i + 1]), __ldg(sp.tw + r * m + slot));
+                }
+            }
+        }
+        tc_fence_before_sync();
+        __syncthreads();
+    }
+    // radix-R DFT over r of every (slot, column pair): rows R * slot + r, no twiddles
+    const int npair = wt >> 1;
+    fft_stage_pair_dispatch<false, false>(R, s, a.n2, 1, make_fastdiv(1u), npair,
+                                          make_fastdiv(static_cast<unsigned int>(npair)), wt, a.plan2.tw, tid, nthr);
+    __syncthreads();
+    return true;
+}
+
+__global__ void __launch_bounds__(512, 1) k_az_rd_split(AzRdArgs a, AzRdSplit sp, unsigned int* err,
+                                                        const __grid_constant__ CUtensorMap map) {
+    extern __shared__ __align__(1024) unsigned char smem_rds_raw[];
+    unsigned char* a_hi = smem_rds_raw;
+    unsigned char* a_lo = a_hi + kSplitOperandBytes;
+    unsigned char* b_hi = a_lo + kSplitOperandBytes;
+    unsigned char* b_lo = b_hi + kSplitMatrixBytes;
+    float2* s = reinterpret_cast<float2*>(b_lo + kSplitMatrixBytes);
+    const int wt = a.wt;
+    ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * wt);
+    int* fbin = reinterpret_cast<int*>(cps + a.xt);
+    __shared__ uint64_t bar, mbar;
+    __shared__ uint32_t tmem_base;
+    if (threadIdx.x < 32) tmem_alloc(&tmem_base, 64);
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, static_cast<uint32_t>(sizeof(float2) * a.n2 * wt));
+        const int x = 2 * (static_cast<int>(blockIdx.x) * a.xt - a.hl);
+        for (int r0 = 0; r0 < a.n2; r0 += a.n2_box)
+            tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
+    }
+    // the DFT matrix images and the column / row tables while the tile is in flight
+    const uint4* bsrc = reinterpret_cast<const uint4*>(sp.bmat);
+    uint4* bdst = reinterpret_cast<uint4*>(b_hi);
+    for (int i = threadIdx.x; i < 2 * kSplitMatrixBytes / 16; i += blockDim.x) bdst[i] = __ldg(bsrc + i);
+    az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbin);
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    mbar_wait(&bar, 0, err);
+    uint32_t phase = 0;
+    if (split_forward(a, sp, s, a_hi, a_lo, b_hi, b_lo, tmem, &mbar, phase, err))
+        az_rd_body<false>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, true);
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    if (threadIdx.x < 32) tmem_dealloc(tmem, 64);
+}
+
 __global__ void __launch_bounds__(512, 2) k_tail(TailArgs a, unsigned int* err) {
     extern __shared__ float smem_tail[];
     tail_body(a, blockIdx.x, threadIdx.x, blockDim.x, smem_tail, err);
@@ -319,6 +447,15 @@ int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, L
     if (rc) return rc;
     k_az_rd<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, err, tmap_or_zero(tmap));
     return check_launch("az_rd");
+}
+
+int backend_az_rd_split(const AzRdArgs& a, const AzRdSplit& sp, const void* tmap, int tiles, int nblocks,
+                        LaunchShape sh, unsigned int* err, void* stream) {
+    if (!tmap) return set_error(ASARF_ERR_INVALID, "az_rd_split: needs the TMA tile loads");
+    int rc = ensure_smem(k_az_rd_split, sh.smem, "az_rd_split");
+    if (rc) return rc;
+    k_az_rd_split<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, sp, err, tmap_or_zero(tmap));
+    return check_launch("az_rd_split");
 }
 
 int backend_make_tmap(void* out, int rank, void* base, const unsigned long long* dims,

@@ -175,6 +175,25 @@ struct AzRdArgs {
     int n2_box;           // rows per TMA box
 };
 
+// Split-precision form of the range-Doppler block's forward transform: n2 = radix * m,
+// m-point DFTs on the tensor cores, one FP32 radix pass (tc.cuh, k_az_rd_split).
+constexpr int kSplitK = 64;          // K of the DFT tile: m <= 32 complex inputs as (re, im) pairs
+constexpr int kSplitN = 64;          // N: m <= 32 complex outputs as (re, im) pairs
+constexpr int kSplitRows = 128;      // M: range columns of the tile (wt <= 128)
+constexpr int kSplitOperandBytes = kSplitRows * kSplitK * 2;   // one bf16 A part (16 KB)
+constexpr int kSplitMatrixBytes = kSplitN * kSplitK * 2;       // one bf16 B part (8 KB)
+// Byte offset of element (row, k) of a 16-bit tensor-core operand with K elements per row in
+// the canonical no-swizzle K-major layout (8 x 8 core matrices of 128 contiguous bytes; K-adjacent
+// core matrices 128 bytes apart, row-adjacent groups 16 K bytes apart).
+ASARF_HD ASARF_INLINE unsigned int umma_offset(int row, int k, int kdim) {
+    return static_cast<unsigned int>((row >> 3) * (kdim * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+struct AzRdSplit {
+    const unsigned char* bmat;  // B hi then lo, canonical K-major images (2 x kSplitMatrixBytes)
+    const float2* tw;           // [radix][m]: W_n2^(r * k1(s)) for output slot s
+    int radix, m;
+};
+
 struct TailVariant {
     int n_lines;
     int out_az;

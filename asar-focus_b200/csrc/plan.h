@@ -56,6 +56,9 @@ struct asarf_plan {
     AzStridedArgs a_fwd{}, a_inv{};
     AzRdArgs a_rd{};
     TailArgs a_tail{};
+    asarf::AzRdSplit a_split{};   // split-precision form of the range-Doppler block (opt.precision)
+    bool split = false;
+    LaunchShape sh_rd_split{};
     int stats_gy = 0;
     LaunchShape sh_rc{}, sh_st{}, sh_rd{}, sh_tail{};
     int tiles1 = 0, tiles2 = 0;

@@ -71,6 +71,12 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi's start-up holds driver locks that stall allocating CUDA calls (the
+        # reference allocates in every step): time nothing until its first sample is in
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10.0:
+            time.sleep(0.05)
+        time.sleep(0.3)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -228,7 +234,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     lib = asarf.load_library()
     sc = make_scene(args.workload, 1001 + rank)
     sc.prepare(lib)
-    plan = asarf.FocusPlan(sc, lib=lib)
+    prec = 1 if args.precision == "split" else 0
+    plan = asarf.FocusPlan(sc, lib=lib, precision=prec)
     raw_np, _ = sim.simulate(sc, device="cuda")
     raw_d = torch.from_numpy(raw_np).cuda()
     out_d = torch.empty(plan.out_shape, dtype=torch.float32, device="cuda")
@@ -267,7 +274,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     # end to end through the public host API: pinned raw in, detected image out, every step.
     # Scenes go round-robin to E2E_DEPTH plans, each on its own stream, so that one scene's
     # upload and another's download overlap a third's focusing (asarf_focus_host_async).
-    plans = [plan] + [asarf.FocusPlan(sc, lib=lib) for _ in range(E2E_DEPTH - 1)]
+    plans = [plan] + [asarf.FocusPlan(sc, lib=lib, precision=prec) for _ in range(E2E_DEPTH - 1)]
     raw_h = [torch.from_numpy(raw_np).pin_memory() for _ in range(E2E_DEPTH)]
     out_h = [torch.empty(plan.out_shape, dtype=torch.float32).pin_memory() for _ in range(E2E_DEPTH)]
     slot_streams = [torch.cuda.Stream() for _ in range(E2E_DEPTH)]
@@ -331,7 +338,9 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                    "l2": f"inputs larger than L2 (raw {raw_np.nbytes / 1e6:.0f} MB, complex images "
                          f"{dims['az_pad'] * dims['nk'] * 8 / 1e9:.2f} GB each)",
                    "parallelism": f"replicas x{world} (independent scenes)",
-                   "az_pad": dims["az_pad"], "rc_fft_len": dims["rc_fft_len"]},
+                   "az_pad": dims["az_pad"], "rc_fft_len": dims["rc_fft_len"],
+                   "precision": "split (tensor-core bf16 hi+lo DFT tiles, FP32 accumulate)" if dims["precision"]
+                   else "plain FP32"},
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
                 "h2d_bytes_per_step": int(raw_np.nbytes), "d2h_bytes_per_step": int(out_h[0].numel() * 4),
                 "ms_per_step": round(e2e_ms, 4), "steps": e2e_steps,
@@ -601,6 +610,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="ers_full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["fp32", "split"], default="fp32",
+                    help="azimuth transform form: plain FP32, or tensor-core bf16 hi+lo DFT tiles")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

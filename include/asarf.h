@@ -99,7 +99,16 @@ typedef struct asarf_options {
     float calibration;         /* MDS calibration constant (main.cc: process gain / sqrt(scaling factor));
                                   default 1 */
     int32_t sq_stats;          /* 1: also compute the product statistics of the SQ ADS (asarf_results.sq_stats) */
+    int32_t precision;         /* ASARF_PRECISION_* (default ASARF_PRECISION_FP32) */
 } asarf_options;
+
+/* Arithmetic of the azimuth transforms (asarf_options.precision).  The reference runs every
+ * transform through cuFFT in FP32 (sar/range_doppler_algorithm.cu:319-323, 385-389). */
+#define ASARF_PRECISION_FP32 0   /* FP32 mixed-radix transforms on the CUDA cores */
+#define ASARF_PRECISION_SPLIT 1  /* forward contiguous azimuth transform of length n2 = R * m (m <= 32) as
+                                    m-point DFT tiles on the tensor cores (tcgen05, bf16 hi + lo operands,
+                                    three products, FP32 accumulation) and one FP32 radix-R pass; plans
+                                    whose n2 has no such split keep FP32 (asarf_dims.precision) */
 
 /* Output geometry of a plan (both tail variants: the Doppler-centroid sign picks one). */
 typedef struct asarf_dims {
@@ -114,6 +123,8 @@ typedef struct asarf_dims {
     double vr_poly[3];
     size_t device_bytes;       /* device memory held by the plan */
     int64_t out_bytes_max;     /* bytes asarf_focus may write at d_out for the plan's product */
+    int32_t precision;         /* ASARF_PRECISION_* the plan runs (SPLIT falls back to FP32 where n2 does not split) */
+    int32_t split_radix, split_m; /* with SPLIT: n2 = split_radix * split_m */
 } asarf_dims;
 
 /* Per-run results: SARResults (sar/sar_metadata.h:46-55) plus the chosen window. */
