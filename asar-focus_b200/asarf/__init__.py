@@ -43,7 +43,8 @@ class FocusPlan:
 
     def __init__(self, scene: Scene, rc_fft_len: int = 0, ref_compat_stats: bool = True, lib=None,
                  lib_path=None, dc_poly=None, product: int = 0, calibration: float = 1.0,
-                 record_header_bytes: int = 17, sq_stats: bool = False, precision: int = 0):
+                 record_header_bytes: int = 17, sq_stats: bool = False, precision: int = 0,
+                 absolute_phase: bool = False):
         self.lib = lib or load_library(lib_path)
         self.scene = scene
         if scene.vr_poly is None or not scene.osv:
@@ -61,6 +62,7 @@ class FocusPlan:
         opt.record_header_bytes = int(record_header_bytes)
         opt.sq_stats = int(bool(sq_stats))
         opt.precision = int(precision)
+        opt.absolute_phase = int(bool(absolute_phase))
         self.product = int(product)
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_plan_create(C.byref(self._sc), C.byref(opt), C.byref(h)), "plan_create")

@@ -38,7 +38,7 @@ class Options(C.Structure):
     _fields_ = [("rc_fft_len", C.c_int32), ("ref_compat_stats", C.c_int32), ("iq_padding_ref", C.c_int32),
                 ("dc_poly_given", C.c_int32), ("dc_poly", C.c_double * 3), ("product", C.c_int32),
                 ("record_header_bytes", C.c_int32), ("calibration", C.c_float), ("sq_stats", C.c_int32),
-                ("precision", C.c_int32)]
+                ("precision", C.c_int32), ("absolute_phase", C.c_int32)]
 
 
 PRECISION_FP32 = 0

@@ -1065,19 +1065,47 @@ ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& 
     return cmul(out, expj_neg_sum(mf_phase, sh_phase));
 }
 
+// Absolute-phase factor of column x: exp(j phi), phi = 4 pi R0 / lambda + pi dc_off^2 / Ka, in
+// FP64 (4 pi R0 / lambda is about 1.9e8 rad at 850 km; it is reduced modulo 2 pi before the
+// cast).  With it the matched filter is exp(-j pi f^2 / Ka) in the unaliased Doppler
+// frequency times the removal of the carrier phase -4 pi R0 / lambda, so a point target keeps
+// its own phase.  The reference has neither term (sar/range_doppler_algorithm.cu:265-290).
+ASARF_HD ASARF_INLINE float2 az_abs_phase(const AzRdArgs& a, const ColParams& cp, int x) {
+    const double kTwoPi = 6.283185307179586476925286766559;
+    const double r0 = a.slant + static_cast<double>(x) * a.range_spacing;
+    const double d = static_cast<double>(cp.dc_off);
+    const double ph = fmod(fmod(2.0 * kTwoPi * r0 / a.lambda_d, kTwoPi) +
+                           fmod(0.5 * kTwoPi * d * d / static_cast<double>(cp.ka), kTwoPi), kTwoPi);
+    return make_float2(static_cast<float>(cos(ph)), static_cast<float>(sin(ph)));
+}
+
+// Shared-memory tables after the tile: column constants (xt), absolute-phase factors (xt),
+// row frequency bins (n2).
+ASARF_HD ASARF_INLINE float2* az_rd_phase_table(ColParams* cps, const AzRdArgs& a) {
+    return reinterpret_cast<float2*>(cps + a.xt);
+}
+ASARF_HD ASARF_INLINE int* az_rd_bin_table(ColParams* cps, const AzRdArgs& a) {
+    return reinterpret_cast<int*>(az_rd_phase_table(cps, a) + a.xt);
+}
+
 // Per-block tables of the range-Doppler block, built while the tile is in flight: column
-// constants of the xt output columns and the frequency bin of each of the n2 rows.
+// constants of the xt output columns (and their absolute-phase factors when asked for) and
+// the frequency bin of each of the n2 rows.
 ASARF_HD ASARF_INLINE void az_rd_tables(const AzRdArgs& a, int tile, int k1, int tid, int nthr, ColParams* cps,
                                         int* fbin) {
     const int x0 = tile * a.xt;
-    for (int c = tid; c < a.xt; c += nthr) cps[c] = az_col_params(a, x0 + c);
+    float2* phs = az_rd_phase_table(cps, a);
+    for (int c = tid; c < a.xt; c += nthr) {
+        cps[c] = az_col_params(a, x0 + c);
+        if (a.absolute_phase) phs[c] = az_abs_phase(a, cps[c], x0 + c);
+    }
     for (int p = tid; p < a.n2; p += nthr) fbin[p] = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
 }
 
-// Shared-memory bytes of the range-Doppler block: tile, column constants, row bins.
+// Shared-memory bytes of the range-Doppler block: tile, column constants, phase factors, row bins.
 inline size_t az_rd_smem(int n2, int wt, int xt) {
     return sizeof(float2) * static_cast<size_t>(n2) * wt + sizeof(ColParams) * static_cast<size_t>(xt) +
-           sizeof(int) * static_cast<size_t>(n2) + 16;
+           sizeof(float2) * static_cast<size_t>(xt) + sizeof(int) * static_cast<size_t>(n2) + 16;
 }
 
 // Right range halo of the range-Doppler block: the taps used (1 .. 14 of 16) reach 6 columns
@@ -1145,6 +1173,11 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
             const int c0 = lane, c1 = lane + 32;
             if (c0 < a.xt && x0 + c0 < a.nk) v0 = rcmc_mf_sample(a, cp0, x0 + c0, f, srow, a.hl + c0, err_flag);
             if (c1 < a.xt && x0 + c1 < a.nk) v1 = rcmc_mf_sample(a, cp1, x0 + c1, f, srow, a.hl + c1, err_flag);
+            if (a.absolute_phase) {
+                const float2* phs = az_rd_phase_table(const_cast<ColParams*>(cps), a);
+                if (c0 < a.xt) v0 = cmul(v0, phs[c0]);
+                if (c1 < a.xt) v1 = cmul(v1, phs[c1]);
+            }
             __syncwarp();
             if (c0 < a.xt) s[p * wt + a.hl + c0] = v0;
             if (c1 < a.xt) s[p * wt + a.hl + c1] = v1;
@@ -1157,9 +1190,11 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
         float2 rowbuf[64];
         for (int p = 0; p < n2; ++p) {
             const int f = fbin[p];
-            for (int c = 0; c < a.xt; ++c)
+            for (int c = 0; c < a.xt; ++c) {
                 rowbuf[c] = (x0 + c < a.nk) ? rcmc_mf_sample(a, cps[c], x0 + c, f, s + p * wt, a.hl + c, err_flag)
                                             : make_float2(0.0f, 0.0f);
+                if (a.absolute_phase) rowbuf[c] = cmul(rowbuf[c], az_rd_phase_table(const_cast<ColParams*>(cps), a)[c]);
+            }
             for (int c = 0; c < a.xt; ++c) s[p * wt + a.hl + c] = rowbuf[c];
         }
     }

@@ -93,7 +93,7 @@ int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, Launch
     TileBuf buf(sh.smem + 128);
     float2* s = buf.data();
     ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * a.wt);
-    int* fbin = reinterpret_cast<int*>(cps + a.xt);
+    int* fbin = az_rd_bin_table(cps, a);
     for (int b = 0; b < nblocks; ++b)
         for (int t = 0; t < tiles; ++t) {
             az_rd_tables(a, t, b, 0, 1, cps, fbin);

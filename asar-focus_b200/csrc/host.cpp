@@ -459,6 +459,7 @@ void asarf_default_options(asarf_options* opt) {
     opt->calibration = 1.0f;
     opt->sq_stats = 0;
     opt->precision = ASARF_PRECISION_FP32;
+    opt->absolute_phase = 0;
 }
 
 int32_t asarf_fft_size_above(int32_t v) { return fft_size_above(v); }
@@ -639,6 +640,16 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     p->pitch = (p->nk + 31) / 32 * 32;
     p->xt1 = (p->n1 * 32 * 8 <= 160 * 1024) ? 32 : 16;
     p->xt2 = az_rd_tile_width(p->n2, p->hl, p->hr);
+    if (opt.precision == ASARF_PRECISION_SPLIT) {
+        // the tensor-core transform converts R x wt operand rows in rounds of kSplitBlocks x 128:
+        // the widest even tile width (>= 32) that needs a single round, else the usual width
+        const int R = p->f2.plan.radix[p->f2.plan.nst - 1];
+        for (int xt = p->xt2; xt >= 32; xt -= 2)
+            if (R * (xt + p->hl + p->hr) <= kSplitBlocks * kSplitRows) {
+                p->xt2 = xt;
+                break;
+            }
+    }
 
     // chirp matched filter in the forward transform's output order, scaled by 1/L
     std::vector<std::complex<float>> chirp;
@@ -920,6 +931,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     for (int k = 0; k < 3; ++k) d.vr_poly[k] = static_cast<float>(p->vr_poly[k]);
     d.state = p->state;
     d.win = win;
+    d.absolute_phase = opt.absolute_phase ? 1 : 0;
+    d.lambda_d = s.wavelength;
     p->tiles2 = (p->nk + p->xt2 - 1) / p->xt2;
     p->sh_rd = {512, az_rd_smem(p->n2, d.wt, d.xt)};
 
@@ -993,9 +1006,9 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         const int R = p->f2.plan.radix[p->f2.plan.nst - 1];
         const int m = p->n2 / R;
         const bool radix_ok = R == 2 || R == 3 || R == 4 || R == 5 || R == 7 || R == 8;
-        const size_t smem_split = 2 * static_cast<size_t>(kSplitOperandBytes) + 2 * kSplitMatrixBytes + p->sh_rd.smem;
-        if (p->use_tma && radix_ok && m >= 2 && 2 * m <= kSplitK && d.wt <= kSplitRows &&
-            smem_split <= smem_optin_limit()) {
+        const size_t smem_split =
+            2 * static_cast<size_t>(kSplitBlocks) * kSplitOperandBytes + 2 * kSplitMatrixBytes + p->sh_rd.smem;
+        if (p->use_tma && radix_ok && m >= 2 && 2 * m <= kSplitK && smem_split <= smem_optin_limit()) {
             std::vector<unsigned char> img;
             std::vector<float2> tws;
             split_dft_tables(p->n2, R, p->f2.drev, img, tws);

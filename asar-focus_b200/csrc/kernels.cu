@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
     const int wt = a.wt;
     float2* s = reinterpret_cast<float2*>(smem_rd_raw);
     ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * wt);
-    int* fbin = reinterpret_cast<int*>(cps + a.xt);
+    int* fbin = az_rd_bin_table(cps, a);
     __shared__ uint64_t bar;
     if (a.use_tma && threadIdx.x == 0) {
         mbar_init(&bar, 1);
@@ -179,76 +179,97 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
 
 // ----------------------------------------------------------------------------- split precision
 // Forward transform of the range-Doppler tile on the tensor cores.  Tile s[l][c], l < n2 =
-// R * m, c < wt <= 128.  For each r < R the sub-sequence x[r + R mm] (mm < m) of every column
-// becomes the bf16 hi + lo operand A (row = column c, K = (mm, re / im)), which multiplies the
-// m-point DFT matrix B (hi + lo, output slot s = frequency k1(s)) as Ahi Bhi + Ahi Blo + Alo Bhi
-// with FP32 accumulation in TMEM; the result times W_n2^(r k1(s)) goes back to row r + R s
-// (a row of the same sub-sequence, already consumed).  A radix-R FP32 pass over rows
-// R s .. R s + R - 1 then leaves frequency k1(s) + m k2 at row R s + k2: the digit-reversed
-// order of the FP32 forward transform (k1(s) is read from that transform's order table).
+// R * m, c < wt.  Operand row rho = r * wt + c holds the sub-sequence x[r + R mm] (mm < m) of
+// column c as bf16 hi + lo parts (K = (mm, re / im)); it multiplies the m-point DFT matrix B
+// (hi + lo, output slot s = frequency k1(s)) as Ahi Bhi + Ahi Blo + Alo Bhi with FP32
+// accumulation in TMEM, and the result times W_n2^(r k1(s)) goes back to row r + R s of column
+// c (a row of the same sub-sequence, already consumed).  Up to kSplitBlocks x 128 operand rows
+// are converted, multiplied and read back per round (one round for the tile widths the
+// planner picks where it can).  A radix-R FP32 pass over rows R s .. R s + R - 1 then leaves
+// frequency k1(s) + m k2 at row R s + k2: the digit-reversed order of the FP32 forward
+// transform (k1(s) is read from that transform's order table).
 // Returns false (error bit set, products drained) if a product did not complete in time.
-__device__ bool split_forward(const AzRdArgs& a, const AzRdSplit& sp, float2* s, unsigned char* a_hi_p,
-                              unsigned char* a_lo_p, const unsigned char* b_hi_p, const unsigned char* b_lo_p,
-                              uint32_t tmem, uint64_t* mbar, uint32_t& phase, unsigned int* err) {
+__device__ bool split_forward(const AzRdArgs& a, const AzRdSplit& sp, float2* s, unsigned char* a_hi,
+                              unsigned char* a_lo, const unsigned char* b_hi, const unsigned char* b_lo,
+                              uint32_t tmem, uint64_t* mbar, unsigned int* err) {
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int wt = a.wt, R = sp.radix, m = sp.m;
     const int warp = tid >> 5, lane = tid & 31;
+    const int wt = a.wt, R = sp.radix, m = sp.m;
+    const int rows = R * wt;
+    constexpr int kRound = kSplitBlocks * kSplitRows;
+    const int nkc = (m + 3) >> 2;  // chunks of 4 complex inputs holding data (the rest stay zero)
+    const FastDiv dwt = make_fastdiv(static_cast<unsigned int>(wt));
     constexpr uint32_t kIdesc = umma_idesc_bf16(kSplitRows, kSplitN);
     constexpr uint32_t kSbo = kSplitK * 16;  // 8 rows x K bf16
-    const uint32_t a_hi = smem_u32(a_hi_p), a_lo = smem_u32(a_lo_p);
-    const uint32_t b_hi = smem_u32(b_hi_p), b_lo = smem_u32(b_lo_p);
-    for (int r = 0; r < R; ++r) {
-        // operands: item = (column c, chunk kc of 4 complex inputs = 8 bf16 = 16 bytes)
-        for (int t = tid; t < kSplitRows * (kSplitK / 8); t += nthr) {
-            const int c = t & (kSplitRows - 1), kc = t >> 7;
-            uint32_t hi[4], lo[4];
+    uint32_t phase = 0;
+    for (int g0 = 0; g0 < rows; g0 += kRound) {
+        const int nrow = min(kRound, rows - g0);
+        const int nblk = (nrow + kSplitRows - 1) / kSplitRows;
+        for (int t = tid; t < nblk * kSplitRows * nkc; t += nthr) {
+            const int kc = t / (nblk * kSplitRows), rl = t - kc * (nblk * kSplitRows);
+            const int rho = g0 + rl;
+            uint32_t hi[4] = {0u, 0u, 0u, 0u}, lo[4] = {0u, 0u, 0u, 0u};
+            if (rl < nrow) {
+                const int r = static_cast<int>(fdiv_u(static_cast<unsigned int>(rho), dwt)), c = rho - r * wt;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int mm = 4 * kc + j;
-                float2 v = make_float2(0.0f, 0.0f);
-                if (c < wt && mm < m) v = s[(r + R * mm) * wt + c];
-                split_bf16x2(v.x, v.y, hi[j], lo[j]);
+                for (int j = 0; j < 4; ++j) {
+                    const int mm = 4 * kc + j;
+                    const float2 v = mm < m ? s[(r + R * mm) * wt + c] : make_float2(0.0f, 0.0f);
+                    split_bf16x2(v.x, v.y, hi[j], lo[j]);
+                }
             }
-            const uint32_t off = umma_offset(c, 8 * kc, kSplitK);
-            *reinterpret_cast<uint4*>(a_hi_p + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<uint4*>(a_lo_p + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+            const uint32_t off = static_cast<uint32_t>(kSplitOperandBytes) * (rl >> 7) + umma_offset(rl & 127, 8 * kc, kSplitK);
+            *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
         }
         fence_async_smem();
         tc_fence_before_sync();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after_sync();
+            const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+            for (int b = 0; b < nblk; ++b) {
+                const uint32_t ah = smem_u32(a_hi) + kSplitOperandBytes * b, al = smem_u32(a_lo) + kSplitOperandBytes * b;
+                const uint32_t d = tmem + static_cast<uint32_t>(kSplitN) * b;
 #pragma unroll
-            for (int ks = 0; ks < kSplitK / 16; ++ks) {
-                const uint32_t o = 256u * ks;  // two 128-byte core-matrix columns per k-step
-                const uint64_t dah = umma_smem_desc(a_hi + o, 128, kSbo), dal = umma_smem_desc(a_lo + o, 128, kSbo);
-                const uint64_t dbh = umma_smem_desc(b_hi + o, 128, kSbo), dbl = umma_smem_desc(b_lo + o, 128, kSbo);
-                umma_bf16(tmem, dah, dbh, kIdesc, ks > 0);
-                umma_bf16(tmem, dah, dbl, kIdesc, true);
-                umma_bf16(tmem, dal, dbh, kIdesc, true);
+                for (int ks = 0; ks < kSplitK / 16; ++ks) {
+                    const uint32_t o = 256u * ks;  // two 128-byte core-matrix columns per k-step
+                    const uint64_t dah = umma_smem_desc(ah + o, 128, kSbo), dal = umma_smem_desc(al + o, 128, kSbo);
+                    const uint64_t dbh = umma_smem_desc(bh + o, 128, kSbo), dbl = umma_smem_desc(bl + o, 128, kSbo);
+                    umma_bf16(d, dah, dbh, kIdesc, ks > 0);
+                    umma_bf16(d, dah, dbl, kIdesc, true);
+                    umma_bf16(d, dal, dbh, kIdesc, true);
+                }
             }
             umma_commit(mbar);
         }
         const bool done = mbar_wait(mbar, phase, nullptr);
         if (__syncthreads_or(!done)) {
             if (tid == 0) atomicOr(err, kErrMmaTimeout);
-            mbar_wait(mbar, phase, nullptr);  // give the products in flight one more bounded wait
+            mbar_wait(mbar, phase, nullptr);  // one more bounded wait for the products in flight
             return false;
         }
         phase ^= 1u;
         tc_fence_after_sync();
-        // accumulator rows: warp -> TMEM lanes 32 (w % 4) .., columns 16 (w / 4) .. (8 slots)
-        if (warp < 16) {
+        // accumulators: warp w reads TMEM lanes 32 (w % 4) .. and columns 16 (w / 4) .. (8 slots)
+        {
             const int q = warp & 3, jb = warp >> 2;
-            float v[16];
-            tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + 16u * jb, v);
-            const int c = 32 * q + lane;
-            if (c < wt) {
+            if (8 * jb < m) {  // warp-uniform
+                for (int b = 0; b < nblk; ++b) {
+                    float v[16];
+                    tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + static_cast<uint32_t>(kSplitN * b + 16 * jb), v);
+                    const int rl = 128 * b + 32 * q + lane;
+                    if (rl < nrow) {
+                        const int rho = g0 + rl;
+                        const int r = static_cast<int>(fdiv_u(static_cast<unsigned int>(rho), dwt)), c = rho - r * wt;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const int slot = 8 * jb + i;
-                    if (slot < m)
-                        s[(r + R * slot) * wt + c] = cmul(make_float2(v[2 * i], v[2 * i + 1]), __ldg(sp.tw + r * m + slot));
+                        for (int i = 0; i < 8; ++i) {
+                            const int slot = 8 * jb + i;
+                            if (slot < m)
+                                s[(r + R * slot) * wt + c] =
+                                    cmul(make_float2(v[2 * i], v[2 * i + 1]), __ldg(sp.tw + r * m + slot));
+                        }
+                    }
                 }
             }
         }
@@ -267,16 +288,16 @@ __global__ void __launch_bounds__(512, 1) k_az_rd_split(AzRdArgs a, AzRdSplit sp
                                                         const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(1024) unsigned char smem_rds_raw[];
     unsigned char* a_hi = smem_rds_raw;
-    unsigned char* a_lo = a_hi + kSplitOperandBytes;
-    unsigned char* b_hi = a_lo + kSplitOperandBytes;
+    unsigned char* a_lo = a_hi + kSplitBlocks * kSplitOperandBytes;
+    unsigned char* b_hi = a_lo + kSplitBlocks * kSplitOperandBytes;
     unsigned char* b_lo = b_hi + kSplitMatrixBytes;
     float2* s = reinterpret_cast<float2*>(b_lo + kSplitMatrixBytes);
     const int wt = a.wt;
     ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * wt);
-    int* fbin = reinterpret_cast<int*>(cps + a.xt);
+    int* fbin = az_rd_bin_table(cps, a);
     __shared__ uint64_t bar, mbar;
     __shared__ uint32_t tmem_base;
-    if (threadIdx.x < 32) tmem_alloc(&tmem_base, 64);
+    if (threadIdx.x < 32) tmem_alloc(&tmem_base, kSplitTmemCols);
     if (threadIdx.x == 0) {
         mbar_init(&mbar, 1);
         mbar_init(&bar, 1);
@@ -285,23 +306,29 @@ __global__ void __launch_bounds__(512, 1) k_az_rd_split(AzRdArgs a, AzRdSplit sp
         for (int r0 = 0; r0 < a.n2; r0 += a.n2_box)
             tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
     }
-    // the DFT matrix images and the column / row tables while the tile is in flight
+    // while the tile is in flight: the DFT matrix images, zeros in the operand K chunks that
+    // never carry data (inputs >= m), the column / row tables
     const uint4* bsrc = reinterpret_cast<const uint4*>(sp.bmat);
-    uint4* bdst = reinterpret_cast<uint4*>(b_hi);
-    for (int i = threadIdx.x; i < 2 * kSplitMatrixBytes / 16; i += blockDim.x) bdst[i] = __ldg(bsrc + i);
+    for (int i = threadIdx.x; i < 2 * kSplitMatrixBytes / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(b_hi)[i] = __ldg(bsrc + i);
+    {
+        const int nkc = (sp.m + 3) >> 2;
+        uint4* a0 = reinterpret_cast<uint4*>(a_hi);
+        for (int i = threadIdx.x; i < 2 * kSplitBlocks * kSplitOperandBytes / 16; i += blockDim.x)
+            if (((i >> 3) & 7) >= nkc) a0[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbin);
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
     const uint32_t tmem = tmem_base;
     mbar_wait(&bar, 0, err);
-    uint32_t phase = 0;
-    if (split_forward(a, sp, s, a_hi, a_lo, b_hi, b_lo, tmem, &mbar, phase, err))
+    if (split_forward(a, sp, s, a_hi, a_lo, b_hi, b_lo, tmem, &mbar, err))
         az_rd_body<false>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, true);
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
-    if (threadIdx.x < 32) tmem_dealloc(tmem, 64);
+    if (threadIdx.x < 32) tmem_dealloc(tmem, kSplitTmemCols);
 }
 
 __global__ void __launch_bounds__(512, 2) k_tail(TailArgs a, unsigned int* err) {

@@ -173,6 +173,8 @@ struct AzRdArgs {
     const float* win;     // 16 RCMC window taps
     int use_tma;
     int n2_box;           // rows per TMA box
+    int absolute_phase;   // 1: multiply column x by exp(j (4 pi R0 / lambda + pi dc_off^2 / Ka)) (FP64)
+    double lambda_d;      // wavelength, FP64
 };
 
 // Split-precision form of the range-Doppler block's forward transform: n2 = radix * m,
@@ -182,6 +184,8 @@ constexpr int kSplitN = 64;          // N: m <= 32 complex outputs as (re, im) p
 constexpr int kSplitRows = 128;      // M: range columns of the tile (wt <= 128)
 constexpr int kSplitOperandBytes = kSplitRows * kSplitK * 2;   // one bf16 A part (16 KB)
 constexpr int kSplitMatrixBytes = kSplitN * kSplitK * 2;       // one bf16 B part (8 KB)
+constexpr int kSplitBlocks = 3;      // operand row blocks per round (3 x 128 rows)
+constexpr int kSplitTmemCols = 256;  // kSplitBlocks accumulators of kSplitN columns, power of 2
 // Byte offset of element (row, k) of a 16-bit tensor-core operand with K elements per row in
 // the canonical no-swizzle K-major layout (8 x 8 core matrices of 128 contiguous bytes; K-adjacent
 // core matrices 128 bytes apart, row-adjacent groups 16 K bytes apart).

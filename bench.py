@@ -206,23 +206,136 @@ def _traffic_from_profiles(kernel: str, workload: str):
     return None
 
 
-def cpu_baseline(sc_full, raw_full) -> dict:
-    """The FP64 CPU oracle on a bounded sample: the first 4096 lines of the same scene."""
+def _cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _slc_of(plan, res):
+    import torch
+    d = torch.empty((res["n_lines"], plan.dims["slc_cols"]), dtype=torch.complex64, device="cuda")
+    plan.slc_into(d, stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return d.cpu().numpy()
+
+
+def _rel_rmse(a, b) -> float:
+    import numpy as np
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    return float(np.sqrt(np.mean(np.abs(a - b) ** 2) / np.mean(np.abs(b) ** 2)))
+
+
+def cpu_baseline_and_quality(sc_full, lib, forms: dict) -> tuple[dict, dict]:
+    """The FP64 CPU oracle on a bounded sample of the workload, timed on the host cores: a
+    4096-line scene with the same sensor, chirp, PRF, orbit and Doppler parameters and a 6 x 4
+    point grid (seeded).  Its outputs are also what the quality block compares every GPU form
+    against: detected-intensity and SLC relative RMSE, and per point target the deviation of
+    resolution, PSLR, ISLR and peak phase (the same tolerances the tests hold)."""
     import numpy as np
     from dataclasses import replace
-    from oracle import rda
+    import asarf
+    from asarf import sim
+    from oracle import irf, rda
     lines = 4096
-    sc = replace(sc_full, azimuth_size=lines)
-    sc.vr_poly = sc_full.vr_poly
-    raw = np.ascontiguousarray(raw_full[:lines])
+    sc = replace(sc_full, azimuth_size=lines, grid=(6, 4), osv=[], vr_poly=None, seed=sc_full.seed + 7)
+    sc.prepare(lib)
+    raw, truth = sim.simulate(sc, device="cuda")
     t0 = time.perf_counter()
-    rda.focus(raw, sc.to_dict())
+    ref = rda.focus(raw, sc.to_dict())
     dt = time.perf_counter() - t0
     n = sc.range_size * lines
-    return {"value": round(n / dt / 1e6, 3), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-            "sample": f"first {lines} lines of the {sc_full.range_size}x{sc_full.azimuth_size} scene "
+    base = {"value": round(n / dt / 1e6, 3), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+            "cpu_model": _cpu_model(),
+            "sample": f"{sc.range_size} x {lines} scene with the workload's parameters and a 6x4 point grid "
                       f"({n / 1e6:.1f} Msamples) through the numpy FP64 oracle (scipy.fft workers=all cores), "
                       f"{dt:.1f} s"}
+    quality = {}
+    for name, prec in forms.items():
+        plan = asarf.FocusPlan(sc, lib=lib, precision=prec)
+        out = plan.focus_host(raw)
+        res = plan.results()
+        slc = _slc_of(plan, res)
+        q = {"detected_rel_rmse": _rel_rmse(out, ref.detected), "slc_rel_rmse": _rel_rmse(slc, ref.slc),
+             "res_rel_max": 0.0, "pslr_db_max": 0.0, "islr_db_max": 0.0, "phase_mrad_max": 0.0, "targets": 0}
+        first = res["first_line"]
+        for (xt, yt) in truth["targets"]:
+            y, x = yt - first, xt - 8
+            if not (40 <= y < slc.shape[0] - 40 and 40 <= x < slc.shape[1] - 40):
+                continue
+            lo, hi = int(max(0, y - 400)), int(min(slc.shape[0], y + 400))
+            blk = np.abs(ref.slc[lo:hi, int(x) - 6:int(x) + 7])
+            py, px = np.unravel_index(np.argmax(blk), blk.shape)
+            a = irf.analyse(slc, lo + py, int(x) - 6 + px)
+            b = irf.analyse(ref.slc, lo + py, int(x) - 6 + px)
+            if not a or not b:
+                continue
+            d = irf.compare(a, b)
+            q["res_rel_max"] = max(q["res_rel_max"], d["res_az_rel"], d["res_rg_rel"])
+            q["pslr_db_max"] = max(q["pslr_db_max"], d["pslr_az_db"], d["pslr_rg_db"])
+            q["islr_db_max"] = max(q["islr_db_max"], d["islr_db"])
+            q["phase_mrad_max"] = max(q["phase_mrad_max"], 1e3 * d["phase_rad"])
+            q["targets"] += 1
+        q = {k: (float(f"{v:.3g}") if isinstance(v, float) else v) for k, v in q.items()}
+        q["precision"] = "split" if plan.dims["precision"] else "fp32"
+        quality[name] = q
+        plan.close()
+    quality["against"] = ("FP64 oracle on the " + base["sample"].split(" through")[0] +
+                          "; tolerances: rel. RMSE 1e-4, resolution 1 %, PSLR 0.1 dB, ISLR 0.2 dB, phase 1 mrad")
+    return base, quality
+
+
+def _e2e_leg(args, sc, plan, lib, raw_np, prec, stream, st, world):
+    """End to end through the public host API: pinned raw in, detected image out, every step.
+    Scenes go round-robin to E2E_DEPTH plans, each on its own stream, so that one scene's
+    upload and another's download overlap a third's focusing (asarf_focus_host_async)."""
+    import torch
+    import asarf
+    samples = sc.range_size * sc.azimuth_size
+    plans = [plan] + [asarf.FocusPlan(sc, lib=lib, precision=prec) for _ in range(E2E_DEPTH - 1)]
+    raw_h = [torch.from_numpy(raw_np).pin_memory() for _ in range(E2E_DEPTH)]
+    out_h = [torch.empty(plan.out_shape, dtype=torch.float32).pin_memory() for _ in range(E2E_DEPTH)]
+    slot_streams = [torch.cuda.Stream() for _ in range(E2E_DEPTH)]
+    for k in range(E2E_DEPTH):
+        plans[k].focus_host_async(raw_h[k].data_ptr(), out_h[k].data_ptr(), stream=slot_streams[k].cuda_stream)
+    torch.cuda.synchronize()
+    for p_ in plans:
+        if p_.results()["errors"]:
+            raise RuntimeError("host run reported error flags")
+    # as many scenes as the timed device steps (at least 30): the pipeline's fill and drain
+    # (one scene's focusing and download) spread over the whole run
+    e2e_steps = max(30, args.steps)
+    _barrier(world)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for s_ in slot_streams:
+        s_.wait_event(t0)
+    for i in range(e2e_steps):
+        k = i % E2E_DEPTH
+        plans[k].focus_host_async(raw_h[k].data_ptr(), out_h[k].data_ptr(), stream=slot_streams[k].cuda_stream)
+    for s_ in slot_streams:
+        stream.wait_stream(s_)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = _max_over_ranks(t0.elapsed_time(t1) / e2e_steps, world)
+    e2e_value = samples * world / e2e_ms / 1e3
+    # the blocking call, one scene at a time (latency of a single scene), for comparison
+    b0 = torch.cuda.Event(enable_timing=True)
+    b1 = torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    for _ in range(3):
+        plan.focus_host_ptr(raw_h[0].data_ptr(), out_h[0].data_ptr(), stream=st)
+    b1.record(stream)
+    torch.cuda.synchronize()
+    blocking_ms = _max_over_ranks(b0.elapsed_time(b1) / 3, world)
+    del plans[1:]
+    return e2e_value, e2e_ms, blocking_ms, out_h
 
 
 def run_ours(args, rank: int, world: int, local: int) -> None:
@@ -271,47 +384,48 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     samples = sc.range_size * sc.azimuth_size
     value = samples * world / ms_max / 1e3
 
-    # end to end through the public host API: pinned raw in, detected image out, every step.
-    # Scenes go round-robin to E2E_DEPTH plans, each on its own stream, so that one scene's
-    # upload and another's download overlap a third's focusing (asarf_focus_host_async).
-    plans = [plan] + [asarf.FocusPlan(sc, lib=lib, precision=prec) for _ in range(E2E_DEPTH - 1)]
-    raw_h = [torch.from_numpy(raw_np).pin_memory() for _ in range(E2E_DEPTH)]
-    out_h = [torch.empty(plan.out_shape, dtype=torch.float32).pin_memory() for _ in range(E2E_DEPTH)]
-    slot_streams = [torch.cuda.Stream() for _ in range(E2E_DEPTH)]
-    for k in range(E2E_DEPTH):
-        plans[k].focus_host_async(raw_h[k].data_ptr(), out_h[k].data_ptr(), stream=slot_streams[k].cuda_stream)
-    torch.cuda.synchronize()
-    for p_ in plans:
-        if p_.results()["errors"]:
-            raise RuntimeError("host run reported error flags")
-    # as many scenes as the timed device steps (at least 30): the pipeline's fill and drain
-    # (one scene's focusing and download) spread over the whole run
-    e2e_steps = max(30, args.steps)
-    _barrier(world)
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    for s_ in slot_streams:
-        s_.wait_event(t0)
-    for i in range(e2e_steps):
-        k = i % E2E_DEPTH
-        plans[k].focus_host_async(raw_h[k].data_ptr(), out_h[k].data_ptr(), stream=slot_streams[k].cuda_stream)
-    for s_ in slot_streams:
-        stream.wait_stream(s_)
-    t1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = _max_over_ranks(t0.elapsed_time(t1) / e2e_steps, world)
-    e2e_value = samples * world / e2e_ms / 1e3
-    # the blocking call, one scene at a time (latency of a single scene), for comparison
-    b0 = torch.cuda.Event(enable_timing=True)
-    b1 = torch.cuda.Event(enable_timing=True)
-    b0.record(stream)
-    for _ in range(3):
-        plan.focus_host_ptr(raw_h[0].data_ptr(), out_h[0].data_ptr(), stream=st)
-    b1.record(stream)
-    torch.cuda.synchronize()
-    blocking_ms = _max_over_ranks(b0.elapsed_time(b1) / 3, world)
-    del plans[1:]
+    # the other precision form on the same scene and buffers, for the plain-vs-split comparison
+    forms = {}
+    if not args.no_forms:
+        other = 1 - prec
+        p2 = asarf.FocusPlan(sc, lib=lib, precision=other)
+        for _ in range(args.warmup):
+            p2.focus(raw_d, out_d, stream=st)
+        p2.enable_timing(args.steps)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            p2.focus(raw_d, out_d, stream=st)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        kt2, kr2 = p2.kernel_times()
+        ms2 = _max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+        if p2.results()["errors"]:
+            raise RuntimeError("other precision form reported error flags")
+        for p_, ms_, kt_, kr_ in ((plan, ms_max, ktimes, kruns), (p2, ms2, kt2, kr2)):
+            name = "split" if p_.dims["precision"] else "fp32"
+            forms[name] = {"ms_per_step": round(ms_, 4), "value": round(samples * world / ms_ / 1e3, 1),
+                           "az_rd_ms": round(kt_["az_rd"] / max(kr_, 1), 4)}
+            if p_.dims["precision"]:
+                forms[name]["split"] = f"n2 = {p_.dims['split_radix']} x {p_.dims['split_m']}"
+        p2.close()
+        del p2
+        # the focus of the other form overwrote out_d: run the headline form once more
+        plan.focus(raw_d, out_d, stream=st)
+        torch.cuda.synchronize()
+
+    e2e = None
+    if not args.no_e2e:
+        e2e_value, e2e_ms, blocking_ms, out_h = _e2e_leg(args, sc, plan, lib, raw_np, prec, stream, st, world)
+        e2e = {"value": round(e2e_value, 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(raw_np.nbytes), "d2h_bytes_per_step": int(out_h[0].numel() * 4),
+               "ms_per_step": round(e2e_ms, 4), "steps": max(30, args.steps),
+               "api": f"asarf_focus_host_async, scenes round-robin over {E2E_DEPTH} plans on their own "
+                      f"streams, pinned host buffers (copies overlap focusing)",
+               "blocking_ms_per_step": round(blocking_ms, 4),
+               "blocking_value": round(samples * world / blocking_ms / 1e3, 1),
+               "blocking_api": "asarf_focus_host, one scene at a time (upload, focus, download serialised)"}
 
     res = plan.results()
     dims = plan.dims
@@ -341,26 +455,20 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                    "az_pad": dims["az_pad"], "rc_fft_len": dims["rc_fft_len"],
                    "precision": "split (tensor-core bf16 hi+lo DFT tiles, FP32 accumulate)" if dims["precision"]
                    else "plain FP32"},
-        "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
-                "h2d_bytes_per_step": int(raw_np.nbytes), "d2h_bytes_per_step": int(out_h[0].numel() * 4),
-                "ms_per_step": round(e2e_ms, 4), "steps": e2e_steps,
-                "api": f"asarf_focus_host_async, scenes round-robin over {E2E_DEPTH} plans on their own "
-                       f"streams, pinned host buffers (copies overlap focusing)",
-                "blocking_ms_per_step": round(blocking_ms, 4),
-                "blocking_value": round(samples * world / blocking_ms / 1e3, 1),
-                "blocking_api": "asarf_focus_host, one scene at a time (upload, focus, download serialised)"},
+        "e2e": e2e,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
                      "algorithmic_bytes_per_launch": int(alg[dom]), "ms_per_launch": round(per_launch[dom], 4)},
         "pipeline_roofline": {"algorithmic_bytes": int(pipe), "achieved": round(pipe / (ms_max * 1e-3) / 1e9, 1),
                               "frac": round(pipe / (ms_max * 1e-3) / 1e9 / peak, 4), "unit": "GB/s"},
         "kernel_ms_per_step": {k: round(v, 4) for k, v in per_launch.items()},
+        "forms": forms or None,
         "gpu_launches": 7 * args.steps,
         "native_libs_mapped": _mapped_native_libs(),
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sc, raw_np)
+        line["cpu_baseline"], line["quality"] = cpu_baseline_and_quality(sc, lib, {"fp32": 0, "split": 1})
     print(json.dumps(line), flush=True)
 
 
@@ -610,6 +718,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="ers_full")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API leg (profiling runs)")
+    ap.add_argument("--no-forms", action="store_true", help="skip timing the other precision form")
     ap.add_argument("--precision", choices=["fp32", "split"], default="fp32",
                     help="azimuth transform form: plain FP32, or tensor-core bf16 hi+lo DFT tiles")
     args = ap.parse_args()

@@ -100,6 +100,11 @@ typedef struct asarf_options {
                                   default 1 */
     int32_t sq_stats;          /* 1: also compute the product statistics of the SQ ADS (asarf_results.sq_stats) */
     int32_t precision;         /* ASARF_PRECISION_* (default ASARF_PRECISION_FP32) */
+    int32_t absolute_phase;    /* 1: zero-Doppler phase preserved: the azimuth matched filter also carries
+                                  exp(j 4 pi R0 / lambda) (R0 = slant range of the column, FP64 on the GPU,
+                                  reduced modulo 2 pi) and exp(j pi dc_off^2 / Ka); 0 (default): the
+                                  reference's convention, whose SLC phase keeps -4 pi R0 / lambda
+                                  (sar/range_doppler_algorithm.cu:265-290) */
 } asarf_options;
 
 /* Arithmetic of the azimuth transforms (asarf_options.precision).  The reference runs every

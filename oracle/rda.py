@@ -395,6 +395,7 @@ class RdaArgs:
     slant_range: float
     dc_poly: np.ndarray
     vr_poly: np.ndarray
+    absolute_phase: bool = False
 
 
 def _bin_freq(az_pad: int, step32):
@@ -436,26 +437,36 @@ def rcmc(src: np.ndarray, nk: int, args: RdaArgs) -> np.ndarray:
     win = blackman16()
     x = np.arange(nk)
     shift, walk = rcmc_shift(args, az_pad, x)
-    calc = x[None, :] + walk
-    valid = (calc - 8 >= 0) & (calc + 8 < nk)
-    off = ((shift - walk.astype(np.float32)).astype(np.float32) + F32(8)).astype(np.float32)
-    acc = np.zeros((az_pad, nk), dtype=np.complex128)
-    norm = np.zeros((az_pad, nk), dtype=np.float64)
-    rows = np.arange(az_pad)[:, None]
-    for i in range(16):
-        arg = (off - F32(i)).astype(np.float32)
-        pa = (PI32 * arg).astype(np.float32)
+
+    def rows_block(r0: int, r1: int) -> None:
+        # every output row reads its own frequency row only: blocks of rows are independent
+        sh, wk = shift[r0:r1], walk[r0:r1]
+        calc = x[None, :] + wk
+        valid = (calc - 8 >= 0) & (calc + 8 < nk)
+        off = ((sh - wk.astype(np.float32)).astype(np.float32) + F32(8)).astype(np.float32)
+        acc = np.zeros((r1 - r0, nk), dtype=np.complex128)
+        norm = np.zeros((r1 - r0, nk), dtype=np.float64)
+        rows = np.arange(r0, r1)[:, None]
+        for i in range(16):
+            arg = (off - F32(i)).astype(np.float32)
+            pa = (PI32 * arg).astype(np.float32)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                s = (np.sin(pa.astype(np.float64)).astype(np.float32) / pa).astype(np.float32)
+            s = np.where(arg == 0, F32(1), s)
+            w = (win[i] * s).astype(np.float32)
+            w = np.where(valid, w, F32(0))
+            col = np.clip(calc - 8 + i, 0, rg_pad - 1)
+            acc += src[rows, col].astype(np.complex128) * w
+            norm += w
         with np.errstate(invalid="ignore", divide="ignore"):
-            s = (np.sin(pa.astype(np.float64)).astype(np.float32) / pa).astype(np.float32)
-        s = np.where(arg == 0, F32(1), s)
-        w = (win[i] * s).astype(np.float32)
-        w = np.where(valid, w, F32(0))
-        col = np.clip(calc - 8 + i, 0, rg_pad - 1)
-        acc += src[rows, col].astype(np.complex128) * w
-        norm += w
-    with np.errstate(invalid="ignore", divide="ignore"):
-        res = np.where(norm != 0, acc / np.where(norm != 0, norm, 1), 0)
-    out[:, :nk] = res.astype(np.complex64)
+            res = np.where(norm != 0, acc / np.where(norm != 0, norm, 1), 0)
+        out[r0:r1, :nk] = res.astype(np.complex64)
+
+    # numpy releases the GIL in these element-wise passes: row blocks run on a thread pool
+    from concurrent.futures import ThreadPoolExecutor
+    step = 512
+    with ThreadPoolExecutor(max_workers=_workers()) as ex:
+        list(ex.map(lambda r0: rows_block(r0, min(az_pad, r0 + step)), range(0, az_pad, step)))
     return out
 
 
@@ -487,6 +498,15 @@ def azimuth_filter(az_pad: int, nk: int, args: RdaArgs) -> np.ndarray:
     mf_phase = (((PI32 * fc).astype(np.float32) * fc).astype(np.float32) / ka).astype(np.float32)
     sh_phase = (((F32(2) * PI32) * (dc_off / ka).astype(np.float32)).astype(np.float32) * bf).astype(np.float32)
     mf = np.exp(-1j * mf_phase.astype(np.float64)) * np.exp(-1j * sh_phase.astype(np.float64))
+    if args.absolute_phase:
+        # the range-dependent azimuth reference phase 4 pi R0 / lambda (about 1.9e8 rad at
+        # 850 km), reduced modulo 2 pi in FP64: no term of this kind exists in the reference
+        # (sar/range_doppler_algorithm.cu:265-290), whose SLC phase keeps -4 pi R0 / lambda
+        ph = np.fmod(4.0 * np.pi * r0 / float(args.wavelength), 2.0 * np.pi)
+        # and the constant the Doppler-centroid shift leaves, pi dc_off^2 / Ka: with it the
+        # filter is exp(-j pi f^2 / Ka) in the unaliased frequency, the zero-Doppler phase kept
+        ph = ph + np.fmod(np.pi * dc_off[0].astype(np.float64) ** 2 / ka[0].astype(np.float64), 2.0 * np.pi)
+        mf = mf * np.exp(1j * ph)[None, :]
     return np.where(keep, mf, 0)
 
 
@@ -647,9 +667,11 @@ def focus_strip(raw: np.ndarray, scene: dict, block: int, overlap: int, ref_comp
     return srgr(ml, start, frac), slc
 
 
-def focus(raw: np.ndarray, scene: dict, ref_compat: bool = True, keep_intermediate: bool = False) -> FocusResult:
+def focus(raw: np.ndarray, scene: dict, ref_compat: bool = True, keep_intermediate: bool = False,
+          absolute_phase: bool = False) -> FocusResult:
     """main.cc:233-327 for a scene described by ``scene`` (see ``asarf.scene.Scene.to_dict``):
-    ERS byte-I/Q or ASAR FBAQ4 records."""
+    ERS byte-I/Q or ASAR FBAQ4 records.  ``absolute_phase`` adds the azimuth reference phase
+    4 pi R0 / lambda per range column (not in the reference)."""
     nr = scene["range_size"]
     na = scene["azimuth_size"]
     nc = scene["chirp_samples"]
@@ -679,7 +701,7 @@ def focus(raw: np.ndarray, scene: dict, ref_compat: bool = True, keep_intermedia
     if keep_intermediate:
         extra["rc"] = img[:na, :nk].copy()
     args = RdaArgs(scene["prf"], scene["wavelength"], scene["az_bw_frac"], scene["range_spacing"],
-                   scene["slant_range_first"], dc_poly, vr_poly)
+                   scene["slant_range_first"], dc_poly, vr_poly, absolute_phase)
     out = range_doppler(img, nk, na, args)
     del img
     win = geo.results_window(dc_poly[-1], scene["lines_before"], scene["lines_after"], max(aperture))
