@@ -44,7 +44,7 @@ class FocusPlan:
     def __init__(self, scene: Scene, rc_fft_len: int = 0, ref_compat_stats: bool = True, lib=None,
                  lib_path=None, dc_poly=None, product: int = 0, calibration: float = 1.0,
                  record_header_bytes: int = 17, sq_stats: bool = False, precision: int = 0,
-                 absolute_phase: bool = False):
+                 absolute_phase: bool = False, az_n2: int = 0, az_tile_width: int = 0, strided_tile_width: int = 0):
         self.lib = lib or load_library(lib_path)
         self.scene = scene
         if scene.vr_poly is None or not scene.osv:
@@ -63,6 +63,9 @@ class FocusPlan:
         opt.sq_stats = int(bool(sq_stats))
         opt.precision = int(precision)
         opt.absolute_phase = int(bool(absolute_phase))
+        opt.az_n2 = int(az_n2)
+        opt.az_tile_width = int(az_tile_width)
+        opt.strided_tile_width = int(strided_tile_width)
         self.product = int(product)
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_plan_create(C.byref(self._sc), C.byref(opt), C.byref(h)), "plan_create")

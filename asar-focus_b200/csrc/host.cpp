@@ -460,6 +460,9 @@ void asarf_default_options(asarf_options* opt) {
     opt->sq_stats = 0;
     opt->precision = ASARF_PRECISION_FP32;
     opt->absolute_phase = 0;
+    opt->az_n2 = 0;
+    opt->az_tile_width = 0;
+    opt->strided_tile_width = 0;
 }
 
 int32_t asarf_fft_size_above(int32_t v) { return fft_size_above(v); }
@@ -584,12 +587,20 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         delete p;
         return set_error(ASARF_ERR_INVALID, "range FFT length %d must be >= range_size and 2^a3^b5^c7^d", p->rc_len);
     }
-    // azimuth split N = n1 * n2, n2 = largest divisor <= sqrt(N)
+    // azimuth split N = n1 * n2, n2 = largest divisor <= sqrt(N) unless the caller names one
     {
         const int N = p->az_pad;
         int best = 1;
         for (int d = 1; static_cast<long long>(d) * d <= N; ++d)
             if (N % d == 0) best = d;
+        if (opt.az_n2 > 0) {
+            if (N % opt.az_n2 != 0 || opt.az_n2 < 16 || opt.az_n2 > 256) {
+                delete p;
+                return set_error(ASARF_ERR_INVALID, "az_n2 %d must divide the azimuth FFT size %d and lie in [16, 256]",
+                                 opt.az_n2, N);
+            }
+            best = opt.az_n2;
+        }
         p->n2 = best;
         p->n1 = N / best;
         if (p->n2 < 2) {
@@ -639,8 +650,20 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     }
     p->pitch = (p->nk + 31) / 32 * 32;
     p->xt1 = (p->n1 * 32 * 8 <= 160 * 1024) ? 32 : 16;
+    if (opt.strided_tile_width == 16 || opt.strided_tile_width == 32) p->xt1 = opt.strided_tile_width;
+    else if (opt.strided_tile_width != 0) {
+        delete p;
+        return set_error(ASARF_ERR_INVALID, "strided_tile_width must be 16 or 32");
+    }
     p->xt2 = az_rd_tile_width(p->n2, p->hl, p->hr);
-    if (opt.precision == ASARF_PRECISION_SPLIT) {
+    if (opt.az_tile_width != 0) {
+        if (opt.az_tile_width < 16 || opt.az_tile_width > 64 || (opt.az_tile_width & 1)) {
+            delete p;
+            return set_error(ASARF_ERR_INVALID, "az_tile_width must be even and in [16, 64]");
+        }
+        p->xt2 = opt.az_tile_width;
+    }
+    if (opt.precision == ASARF_PRECISION_SPLIT && opt.az_tile_width == 0) {
         // the tensor-core transform converts R x wt operand rows in rounds of kSplitBlocks x 128:
         // the widest even tile width (>= 32) that needs a single round, else the usual width
         const int R = p->f2.plan.radix[p->f2.plan.nst - 1];
@@ -1062,6 +1085,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     dm.precision = p->split ? ASARF_PRECISION_SPLIT : ASARF_PRECISION_FP32;
     dm.split_radix = p->split ? p->a_split.radix : 0;
     dm.split_m = p->split ? p->a_split.m : 0;
+    dm.az_tile_width = p->xt2;
+    dm.strided_tile_width = p->xt1;
     *out = p;
     return ASARF_OK;
 }

@@ -290,14 +290,14 @@ def cpu_baseline_and_quality(sc_full, lib, forms: dict) -> tuple[dict, dict]:
     return base, quality
 
 
-def _e2e_leg(args, sc, plan, lib, raw_np, prec, stream, st, world):
+def _e2e_leg(args, sc, plan, lib, raw_np, opts, stream, st, world):
     """End to end through the public host API: pinned raw in, detected image out, every step.
     Scenes go round-robin to E2E_DEPTH plans, each on its own stream, so that one scene's
     upload and another's download overlap a third's focusing (asarf_focus_host_async)."""
     import torch
     import asarf
     samples = sc.range_size * sc.azimuth_size
-    plans = [plan] + [asarf.FocusPlan(sc, lib=lib, precision=prec) for _ in range(E2E_DEPTH - 1)]
+    plans = [plan] + [asarf.FocusPlan(sc, lib=lib, **opts) for _ in range(E2E_DEPTH - 1)]
     raw_h = [torch.from_numpy(raw_np).pin_memory() for _ in range(E2E_DEPTH)]
     out_h = [torch.empty(plan.out_shape, dtype=torch.float32).pin_memory() for _ in range(E2E_DEPTH)]
     slot_streams = [torch.cuda.Stream() for _ in range(E2E_DEPTH)]
@@ -348,9 +348,21 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     sc = make_scene(args.workload, 1001 + rank)
     sc.prepare(lib)
     prec = 1 if args.precision == "split" else 0
-    plan = asarf.FocusPlan(sc, lib=lib, precision=prec)
     raw_np, _ = sim.simulate(sc, device="cuda")
     raw_d = torch.from_numpy(raw_np).cuda()
+    # launch shapes: timed autotuner (a fresh cache per run, so every run tunes on its own GPU)
+    tuned, tune_info = {}, None
+    if not args.no_tune:
+        import tempfile
+        from asarf import autotune
+        with tempfile.TemporaryDirectory() as td:
+            cache = Path(td) / "tune.json"
+            t_tune = time.perf_counter()
+            tuned = autotune.tune(sc, raw_d, lib=lib, precision=prec, cache=cache)
+            entry = json.loads(cache.read_text())[autotune.shape_key(sc, prec)]
+            tune_info = {"options": tuned, "ms_default": round(entry["ms_default"], 4),
+                         "ms_tuned": round(entry["ms_tuned"], 4), "seconds": round(time.perf_counter() - t_tune, 1)}
+    plan = asarf.FocusPlan(sc, lib=lib, **dict(tuned, precision=prec))
     out_d = torch.empty(plan.out_shape, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
     st = stream.cuda_stream
@@ -388,7 +400,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     forms = {}
     if not args.no_forms:
         other = 1 - prec
-        p2 = asarf.FocusPlan(sc, lib=lib, precision=other)
+        p2 = asarf.FocusPlan(sc, lib=lib, precision=other)  # the planner's own launch shapes
         for _ in range(args.warmup):
             p2.focus(raw_d, out_d, stream=st)
         p2.enable_timing(args.steps)
@@ -417,7 +429,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
 
     e2e = None
     if not args.no_e2e:
-        e2e_value, e2e_ms, blocking_ms, out_h = _e2e_leg(args, sc, plan, lib, raw_np, prec, stream, st, world)
+        e2e_value, e2e_ms, blocking_ms, out_h = _e2e_leg(args, sc, plan, lib, raw_np, dict(tuned, precision=prec),
+                                                         stream, st, world)
         e2e = {"value": round(e2e_value, 1), "unit": UNIT,
                "h2d_bytes_per_step": int(raw_np.nbytes), "d2h_bytes_per_step": int(out_h[0].numel() * 4),
                "ms_per_step": round(e2e_ms, 4), "steps": max(30, args.steps),
@@ -454,7 +467,11 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                    "parallelism": f"replicas x{world} (independent scenes)",
                    "az_pad": dims["az_pad"], "rc_fft_len": dims["rc_fft_len"],
                    "precision": "split (tensor-core bf16 hi+lo DFT tiles, FP32 accumulate)" if dims["precision"]
-                   else "plain FP32"},
+                   else "plain FP32",
+                   "launch_shapes": {"az_n2": dims["n2"], "az_tile_width": dims["az_tile_width"],
+                                     "strided_tile_width": dims["strided_tile_width"],
+                                     "rc_fft_len": dims["rc_fft_len"]},
+                   "autotune": tune_info},
         "e2e": e2e,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
@@ -720,6 +737,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API leg (profiling runs)")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other precision form")
+    ap.add_argument("--no-tune", action="store_true", help="the planner's launch shapes, no timed autotuning")
     ap.add_argument("--precision", choices=["fp32", "split"], default="fp32",
                     help="azimuth transform form: plain FP32, or tensor-core bf16 hi+lo DFT tiles")
     args = ap.parse_args()

@@ -105,6 +105,12 @@ typedef struct asarf_options {
                                   reduced modulo 2 pi) and exp(j pi dc_off^2 / Ka); 0 (default): the
                                   reference's convention, whose SLC phase keeps -4 pi R0 / lambda
                                   (sar/range_doppler_algorithm.cu:265-290) */
+    /* launch shapes (0 = the planner's choice; asarf.autotune times candidates and caches the best
+     * per scene shape): */
+    int32_t az_n2;             /* contiguous azimuth transform length n2 (az_pad = n1 * n2; a divisor of az_pad,
+                                  16 <= n2 <= 256) */
+    int32_t az_tile_width;     /* output range columns per range-Doppler block (even, 16..64) */
+    int32_t strided_tile_width; /* range columns per strided-pass block (16 or 32) */
 } asarf_options;
 
 /* Arithmetic of the azimuth transforms (asarf_options.precision).  The reference runs every
@@ -130,6 +136,7 @@ typedef struct asarf_dims {
     int64_t out_bytes_max;     /* bytes asarf_focus may write at d_out for the plan's product */
     int32_t precision;         /* ASARF_PRECISION_* the plan runs (SPLIT falls back to FP32 where n2 does not split) */
     int32_t split_radix, split_m; /* with SPLIT: n2 = split_radix * split_m */
+    int32_t az_tile_width, strided_tile_width; /* launch shapes in use */
 } asarf_dims;
 
 /* Per-run results: SARResults (sar/sar_metadata.h:46-55) plus the chosen window. */
