@@ -44,7 +44,8 @@ class FocusPlan:
     def __init__(self, scene: Scene, rc_fft_len: int = 0, ref_compat_stats: bool = True, lib=None,
                  lib_path=None, dc_poly=None, product: int = 0, calibration: float = 1.0,
                  record_header_bytes: int = 17, sq_stats: bool = False, precision: int = 0,
-                 absolute_phase: bool = False, az_n2: int = 0, az_tile_width: int = 0, strided_tile_width: int = 0):
+                 absolute_phase: bool = False, az_n2: int = 0, az_tile_width: int = 0, strided_tile_width: int = 0,
+                 keep_slc: bool = True):
         self.lib = lib or load_library(lib_path)
         self.scene = scene
         if scene.vr_poly is None or not scene.osv:
@@ -66,6 +67,7 @@ class FocusPlan:
         opt.az_n2 = int(az_n2)
         opt.az_tile_width = int(az_tile_width)
         opt.strided_tile_width = int(strided_tile_width)
+        opt.keep_slc = int(bool(keep_slc))
         self.product = int(product)
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_plan_create(C.byref(self._sc), C.byref(opt), C.byref(h)), "plan_create")
@@ -197,7 +199,10 @@ class FocusBatch:
     kernels in one CUDA graph with concurrent branches, replayed on later calls with the same
     buffers.  ``plans[i]`` is segment i's plan (dims, results, SLC)."""
 
-    def __init__(self, scenes, branches: int = 4, ref_compat_stats: bool = True, lib=None, lib_path=None):
+    def __init__(self, scenes, branches: int = 4, ref_compat_stats: bool = True, lib=None, lib_path=None,
+                 precision: int = 0, options=None):
+        """``options``: per-segment dicts of launch shapes (az_n2, az_tile_width,
+        strided_tile_width, rc_fft_len), e.g. from asarf.autotune.tune."""
         self.lib = lib or load_library(lib_path)
         self.scenes = list(scenes)
         n = len(self.scenes)
@@ -210,6 +215,10 @@ class FocusBatch:
         for i in range(n):
             self.lib.asarf_default_options(C.byref(opts[i]))
             opts[i].ref_compat_stats = int(bool(ref_compat_stats))
+            opts[i].precision = int(precision)
+            for k, v in ((options[i] if options else None) or {}).items():
+                if k in ("az_n2", "az_tile_width", "strided_tile_width", "rc_fft_len", "precision", "keep_slc"):
+                    setattr(opts[i], k, int(v))
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_batch_create(arr, n, C.cast(opts, C.c_void_p), int(branches), C.byref(h)),
                    "batch_create")

@@ -39,7 +39,7 @@ class Options(C.Structure):
                 ("dc_poly_given", C.c_int32), ("dc_poly", C.c_double * 3), ("product", C.c_int32),
                 ("record_header_bytes", C.c_int32), ("calibration", C.c_float), ("sq_stats", C.c_int32),
                 ("precision", C.c_int32), ("absolute_phase", C.c_int32), ("az_n2", C.c_int32),
-                ("az_tile_width", C.c_int32), ("strided_tile_width", C.c_int32)]
+                ("az_tile_width", C.c_int32), ("strided_tile_width", C.c_int32), ("keep_slc", C.c_int32)]
 
 
 PRECISION_FP32 = 0

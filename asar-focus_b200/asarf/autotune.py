@@ -76,14 +76,14 @@ def _n2_candidates(az_pad: int, count: int = 4) -> list[int]:
 
 
 def tune(scene, raw_d, lib=None, precision: int = 0, cache=None, runs: int = 4, refresh: bool = False,
-         quick: bool = False) -> dict:
+         quick: bool = False, keep_slc: bool = True) -> dict:
     """Options for FocusPlan (az_n2, az_tile_width, strided_tile_width, rc_fft_len) chosen by
     timing on the current GPU, read from / written to the cache file.  ``raw_d``: the scene's
     raw bytes on the device.  ``quick``: tile widths only (batches of many shapes)."""
     import torch
     lib = lib or _lib.load_library()
     path = Path(cache) if cache else _default_cache()
-    key = shape_key(scene, precision)
+    key = shape_key(scene, precision) + ("" if keep_slc else ":detected-only")
     table = {}
     if path.exists():
         try:
@@ -93,19 +93,22 @@ def tune(scene, raw_d, lib=None, precision: int = 0, cache=None, runs: int = 4, 
     if key in table and not refresh:
         return dict(table[key]["options"])
 
-    base = FocusPlan(scene, lib=lib, precision=precision)
+    base = FocusPlan(scene, lib=lib, precision=precision, keep_slc=keep_slc)
     dims = dict(base.dims)
     out_d = torch.empty(int(math.prod(base.out_shape)) * 2, dtype=torch.float32, device="cuda")
     base.close()
-    best = {"precision": precision}
+    best = {"precision": precision, "keep_slc": bool(keep_slc)}
+    timings = []
     best_ms = _time_options(scene, raw_d, out_d, lib, best, runs)
     default_ms = best_ms
+    timings.append([{}, default_ms])
 
     def sweep(name, values):
         nonlocal best, best_ms
         for v in values:
             trial = dict(best, **{name: v})
             ms = _time_options(scene, raw_d, out_d, lib, trial, runs)
+            timings.append([{k: x for k, x in trial.items() if k not in ("precision", "keep_slc")}, ms])
             if ms is not None and (best_ms is None or ms < best_ms):
                 best, best_ms = trial, ms
 
@@ -117,7 +120,7 @@ def tune(scene, raw_d, lib=None, precision: int = 0, cache=None, runs: int = 4, 
         rc = [L for L in CT_LENGTHS if L >= scene.range_size and 2 * L <= 3 * scene.range_size]
         sweep("rc_fft_len", [L for L in rc if L != dims["rc_fft_len"]])
     opts = {k: v for k, v in best.items()}
-    table[key] = {"options": opts, "ms_default": default_ms, "ms_tuned": best_ms}
+    table[key] = {"options": opts, "ms_default": default_ms, "ms_tuned": best_ms, "timings": timings}
     try:
         path.parent.mkdir(parents=True, exist_ok=True)
         path.write_text(json.dumps(table, indent=1, sort_keys=True))

@@ -943,8 +943,12 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
             const int x = x0 + c;
             if (x < a.nk && row >= lo && row < hi) {
                 const float2 v = s[t];
-                a.out[static_cast<long long>(row - a.out_row0) * a.pitch + x] =
-                    make_float2(fmul_rn(v.x, a.scale), fmul_rn(v.y, a.scale));
+                const float2 u = make_float2(fmul_rn(v.x, a.scale), fmul_rn(v.y, a.scale));
+                const long long o = static_cast<long long>(row - a.out_row0) * a.pitch + x;
+                if (a.out_intensity)
+                    a.out_intensity[o] = fma_rn(u.x, u.x, fmul_rn(u.y, u.y));  // the tail's |z|^2, same rounding
+                else
+                    a.out[o] = u;
             }
         }
     }
@@ -1289,6 +1293,7 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
     const int c0 = e0 > s0 ? e0 - s0 : 0;
     const int c1 = e1 > s1 ? e1 - s1 : 0;
     const float2* base = a.slc + static_cast<long long>(st.first_line) * a.pitch + a.col0;
+    const float* ibase = a.intensity ? a.intensity + static_cast<long long>(st.first_line) * a.pitch + a.col0 : nullptr;
     const int r_lo = s0 < s1 ? s0 : s1;
     const int r_hi = e0 > e1 ? e0 : e1;
     // each input row is read once and added to whichever box mean(s) contain it, in row
@@ -1301,15 +1306,23 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
     // quotients from their correctly rounded reciprocals (div_by_recip_rn)
     const float fc0 = c0 ? static_cast<float>(c0) : 1.0f, fc1 = c1 ? static_cast<float>(c1) : 1.0f;
     const float rc0 = fdiv_rn(1.0f, fc0), rc1 = fdiv_rn(1.0f, fc1);
+    // |z|^2 of row r, column c: from the complex SLC, or read directly from the intensity rows
+    // the inverse azimuth pass wrote for detected products (half the bytes, same rounding)
+    auto power = [&](int r, int c) -> float {
+        const long long o = static_cast<long long>(r) * a.pitch + c;
+        if (ibase) return ibase[o];
+        const float2 w = base[o];
+        return fma_rn(w.x, w.x, fmul_rn(w.y, w.y));
+    };
     for (int cb = tid; cb < a.nx; cb += 2 * nthr) {
-        float2 v[2][kTailRows];
+        float v[2][kTailRows];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int c = cb + h * nthr;
 #pragma unroll
             for (int k = 0; k < kTailRows; ++k) {
-                v[h][k] = make_float2(0.0f, 0.0f);
-                if (k < nr && c < a.nx) v[h][k] = base[static_cast<long long>(r_lo + k) * a.pitch + c];
+                v[h][k] = 0.0f;
+                if (k < nr && c < a.nx) v[h][k] = power(r_lo + k, c);
             }
         }
 #pragma unroll
@@ -1321,13 +1334,11 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
             for (int k = 0; k < kTailRows; ++k) {
                 const int r = r_lo + k;
                 if (k >= nr) break;
-                const float p2 = fma_rn(v[h][k].x, v[h][k].x, fmul_rn(v[h][k].y, v[h][k].y));
-                if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
-                if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
+                if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, v[h][k]);
+                if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, v[h][k]);
             }
             for (int r = r_lo + kTailRows; r < r_hi; ++r) {
-                const float2 w = base[static_cast<long long>(r) * a.pitch + c];
-                const float p2 = fma_rn(w.x, w.x, fmul_rn(w.y, w.y));
+                const float p2 = power(r, c);
                 if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
                 if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
             }

@@ -463,6 +463,7 @@ void asarf_default_options(asarf_options* opt) {
     opt->az_n2 = 0;
     opt->az_tile_width = 0;
     opt->strided_tile_width = 0;
+    opt->keep_slc = 1;
 }
 
 int32_t asarf_fft_size_above(int32_t v) { return fft_size_above(v); }
@@ -959,8 +960,14 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     p->tiles2 = (p->nk + p->xt2 - 1) / p->xt2;
     p->sh_rd = {512, az_rd_smem(p->n2, d.wt, d.xt)};
 
+    // detected products without a kept SLC: the inverse azimuth pass writes |z|^2 rows into
+    // bufA (free once the range-Doppler block has read it) and the tail reads those
+    p->intensity_only = !opt.keep_slc &&
+                        (opt.product == ASARF_PRODUCT_DETECTED || (opt.product == ASARF_PRODUCT_IMP_MDS && !opt.sq_stats));
+    if (p->intensity_only) p->a_inv.out_intensity = reinterpret_cast<float*>(p->bufA);
     TailArgs& t = p->a_tail;
     t.slc = p->bufB;
+    t.intensity = p->intensity_only ? reinterpret_cast<const float*>(p->bufA) : nullptr;
     t.pitch = p->pitch;
     t.state = p->state;
     t.col0 = kRcmcTaps / 2;
@@ -1323,6 +1330,8 @@ int asarf_plan_results(asarf_plan* p, asarf_results* res, void* stream) {
 
 int asarf_plan_slc(asarf_plan* p, void* d_slc, void* stream) {
     if (!p || !d_slc) return set_error(ASARF_ERR_INVALID, "plan_slc: null argument");
+    if (p->intensity_only)
+        return set_error(ASARF_ERR_INVALID, "plan_slc: the plan keeps no complex SLC (asarf_options.keep_slc = 0)");
     FocusState st;
     int rc = mem_d2h(&st, p->state, sizeof(st), stream);
     if (rc) return rc;

@@ -144,6 +144,8 @@ struct AzStridedArgs {
     int use_tma;          // tile loaded by TMA (device only)
     int n1_box;           // rows per TMA box (n1 split into n1 / n1_box boxes of <= 256 rows)
     int out_row0;         // inverse: row r is stored at out + (r - out_row0) * pitch
+    float* out_intensity; // inverse: when set, |z|^2 of row r goes to out_intensity + (r - out_row0) * pitch
+                          // (floats) and no complex row is stored
 };
 
 // Per range column constants of the range-Doppler block.
@@ -209,6 +211,7 @@ struct TailVariant {
 
 struct TailArgs {
     const float2* slc;
+    const float* intensity;  // when set: |z|^2 rows (floats, same pitch) instead of the complex SLC
     long long pitch;
     const FocusState* state;
     int col0, nx;

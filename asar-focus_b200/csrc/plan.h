@@ -75,6 +75,7 @@ struct asarf_plan {
     alignas(64) unsigned char tmapA2[128] = {};
     bool use_tma = false;
     bool skip_tail = false;       // strip blocks: the strip runs one tail over all blocks
+    bool intensity_only = false;  // keep_slc = 0: |z|^2 rows instead of the complex SLC
     int raw_smem_offset = 0;
     // asynchronous host runs: the plan's own non-blocking stream (created on first use) and
     // the event recorded after the last enqueued image download

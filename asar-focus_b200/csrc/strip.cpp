@@ -130,6 +130,8 @@ int asarf_strip_create(const asarf_scene* scene, int32_t block_lines, int32_t ov
         }
         p->a_inv.out = st->slc;
         p->a_inv.out_row0 = st->start_margin - st->start[static_cast<size_t>(k)];
+        p->a_inv.out_intensity = nullptr;  // blocks write their complex share into the strip SLC
+        p->intensity_only = false;
     }
 
     // tail over the whole strip SLC (the planned path's tail with a strip-wide window)

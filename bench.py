@@ -358,10 +358,13 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         with tempfile.TemporaryDirectory() as td:
             cache = Path(td) / "tune.json"
             t_tune = time.perf_counter()
-            tuned = autotune.tune(sc, raw_d, lib=lib, precision=prec, cache=cache)
-            entry = json.loads(cache.read_text())[autotune.shape_key(sc, prec)]
+            tuned = autotune.tune(sc, raw_d, lib=lib, precision=prec, cache=cache, keep_slc=False)
+            entry = json.loads(cache.read_text())[autotune.shape_key(sc, prec) + ":detected-only"]
             tune_info = {"options": tuned, "ms_default": round(entry["ms_default"], 4),
-                         "ms_tuned": round(entry["ms_tuned"], 4), "seconds": round(time.perf_counter() - t_tune, 1)}
+                         "ms_tuned": round(entry["ms_tuned"], 4), "seconds": round(time.perf_counter() - t_tune, 1),
+                         "candidates": [[o, None if m is None else round(m, 4)] for o, m in entry["timings"]]}
+    # the product is the detected image: no complex SLC is kept (|z|^2 rows feed the multilook)
+    tuned = dict(tuned, keep_slc=False)
     plan = asarf.FocusPlan(sc, lib=lib, **dict(tuned, precision=prec))
     out_d = torch.empty(plan.out_shape, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
@@ -400,7 +403,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     forms = {}
     if not args.no_forms:
         other = 1 - prec
-        p2 = asarf.FocusPlan(sc, lib=lib, precision=other)  # the planner's own launch shapes
+        p2 = asarf.FocusPlan(sc, lib=lib, precision=other, keep_slc=False)  # the planner's own launch shapes
         for _ in range(args.warmup):
             p2.focus(raw_d, out_d, stream=st)
         p2.enable_timing(args.steps)
@@ -608,8 +611,20 @@ def run_batch(args, rank: int, world: int, local: int) -> None:
         sc.prepare(lib)
     bins = asarf.lpt_assign([sc.range_size * sc.azimuth_size for sc in scenes], world, lib=lib)
     mine = [i for i, b in enumerate(bins) if b == rank]
-    batch = asarf.FocusBatch([scenes[i] for i in mine], lib=lib)
     raws = [torch.from_numpy(sim.simulate(scenes[i], device="cuda")[0]).cuda() for i in mine]
+    prec = 1 if args.precision == "split" else 0
+    # per-segment launch shapes from the timed autotuner (tile widths: every segment has its own shape)
+    seg_opts, t_tune = None, None
+    if not args.no_tune:
+        import tempfile
+        from asarf import autotune
+        t0 = time.perf_counter()
+        with tempfile.TemporaryDirectory() as td:
+            seg_opts = [autotune.tune(scenes[i], r, lib=lib, precision=prec, cache=Path(td) / "tune.json", quick=True,
+                                      runs=2, keep_slc=False) for i, r in zip(mine, raws)]
+        t_tune = round(time.perf_counter() - t0, 1)
+    batch = asarf.FocusBatch([scenes[i] for i in mine], lib=lib, precision=prec,
+                             options=seg_opts or [{"keep_slc": False}] * len(mine))
     outs = [torch.empty(p.out_shape, dtype=torch.float32, device="cuda") for p in batch.plans]
     stream = torch.cuda.current_stream()
     st = stream.cuda_stream
@@ -638,6 +653,17 @@ def run_batch(args, rank: int, world: int, local: int) -> None:
     clocks = sampler.stop()
     seq_ms = timed(lambda: [p.focus(r, o, stream=st) for p, r, o in zip(batch.plans, raws, outs)],
                    max(3, min(args.steps, 10)))
+    # the other precision form of the same batch (planner's launch shapes), for the comparison
+    other_ms = None
+    if not args.no_forms:
+        b2 = asarf.FocusBatch([scenes[i] for i in mine], lib=lib, precision=1 - prec,
+                              options=[{"keep_slc": False}] * len(mine))
+        for _ in range(args.warmup):
+            b2.focus(raws, outs, stream=st)
+        other_ms = timed(lambda: b2.focus(raws, outs, stream=st), max(3, min(args.steps, 10)))
+        n_split = sum(1 for p in b2.plans if p.dims["precision"])
+        b2.close()
+        del b2
     samples = sum(sc.range_size * sc.azimuth_size for sc in scenes)
     value = samples / ms / 1e3
     peaks = _peaks()
@@ -654,9 +680,16 @@ def run_batch(args, rank: int, world: int, local: int) -> None:
         "vs_baseline": None, "dtype": "fp32 (complex64 data, FP64 geometry)", "data": "synthetic",
         "config": {"workload": "batch16: 16 uneven segments (ERS 5-bit / ASAR 8-bit, range 2048|5616, "
                                "azimuth U[4000, 30000]), one CUDA graph per rank",
+                   "precision": "split" if prec else "plain FP32",
                    "segments": [[sc.range_size, sc.azimuth_size, sc.bits] for sc in scenes],
                    "l2": "inputs larger than L2", "parallelism": f"segments dealt to {world} rank(s) by LPT"},
         "sequential_ms_per_step": round(seq_ms, 4),
+        "forms": None if other_ms is None else {
+            ("split" if prec else "fp32"): {"ms_per_step": round(ms, 4), "value": round(value, 1)},
+            ("fp32" if prec else "split"): {"ms_per_step": round(other_ms, 4),
+                                            "value": round(samples / other_ms / 1e3, 1),
+                                            "segments_on_tensor_cores": n_split if not prec else None}},
+        "autotune": None if seg_opts is None else {"seconds": t_tune, "options": seg_opts},
         "pipeline_roofline": {"algorithmic_bytes": int(pipe), "achieved": round(pipe / (ms * 1e-3) / 1e9, 1),
                               "frac": round(pipe / (ms * 1e-3) / 1e9 / peak, 4), "unit": "GB/s"},
         "gpu_launches": 7 * len(scenes) * args.steps,

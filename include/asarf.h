@@ -111,6 +111,10 @@ typedef struct asarf_options {
                                   16 <= n2 <= 256) */
     int32_t az_tile_width;     /* output range columns per range-Doppler block (even, 16..64) */
     int32_t strided_tile_width; /* range columns per strided-pass block (16 or 32) */
+    int32_t keep_slc;          /* 1 (default): the complex SLC stays in device memory after a run
+                                  (asarf_plan_slc, IMS records, the IMP product statistics);
+                                  0: detected output only -- the inverse azimuth pass writes |z|^2 rows
+                                  (half the bytes written, and read again by the multilook) */
 } asarf_options;
 
 /* Arithmetic of the azimuth transforms (asarf_options.precision).  The reference runs every

@@ -125,3 +125,41 @@ def test_batch_graph_equals_single_plans(gpu_lib):
     third = run(outs2)                     # new buffers: new capture
     for s, a, b, c in zip(singles, first, again, third):
         assert np.array_equal(a, s) and np.array_equal(b, s) and np.array_equal(c, s)
+
+
+@pytest.mark.gpu
+def test_batch16_shapes_equal_single_plans_and_oracle(gpu_lib):
+    """The benchmark's 16 uneven segments (range 2048 | 5616, azimuth 4000..30000, 5- and
+    8-bit) in one graph: every segment bit-identical to its plan run alone, in both precision
+    forms, and the smallest 5616-range segment against the FP64 oracle."""
+    import torch
+    from asarf import sim
+    from conftest import oracle_focus, rel_rmse
+    scenes = S.batch16()
+    for sc in scenes:
+        sc.prepare(gpu_lib)
+    raws_np = [sim.simulate(sc, device="cuda")[0] for sc in scenes]
+    raws = [torch.from_numpy(r).cuda() for r in raws_np]
+    stream = torch.cuda.current_stream().cuda_stream
+    for precision in (0, 1):
+        batch = asarf.FocusBatch(scenes, lib=gpu_lib, precision=precision)
+        outs = [torch.zeros(p.out_shape, dtype=torch.float32, device="cuda") for p in batch.plans]
+        batch.focus(raws, outs, stream=stream)
+        torch.cuda.synchronize()
+        for i, (p, o) in enumerate(zip(batch.plans, outs)):
+            r = p.results()
+            assert r["errors"] == 0, i
+            single = asarf.FocusPlan(scenes[i], lib=gpu_lib, precision=precision)
+            so = torch.zeros(single.out_shape, dtype=torch.float32, device="cuda")
+            single.focus(raws[i], so, stream=stream)
+            torch.cuda.synchronize()
+            assert torch.equal(o[: r["out_rows"], : r["out_cols"]], so[: r["out_rows"], : r["out_cols"]]), i
+            single.close()
+        if precision == 0:
+            k = min((i for i, sc in enumerate(scenes) if sc.range_size == 5616), key=lambda i: scenes[i].azimuth_size)
+            r = batch.plans[k].results()
+            got = outs[k].cpu().numpy()[: r["out_rows"], : r["out_cols"]]
+            ref = oracle_focus(scenes[k], raws_np[k])
+            assert got.shape == ref.detected.shape
+            assert rel_rmse(got, ref.detected) < 1e-5
+        batch.close()

@@ -93,3 +93,16 @@ def test_swst_shift_and_unwindowed_chirp(emu_lib, ref_compat):
     res = plan.results()
     ref = oracle_focus(sc, raw, ref_compat=ref_compat)
     _check(plan, out, res, ref)
+
+
+def test_detected_only_runs_equal_the_kept_slc_runs(emu_lib):
+    """keep_slc = 0: the inverse azimuth pass writes |z|^2 rows and the multilook reads them;
+    the detected image is bit-identical, and the complex SLC is not offered."""
+    from asarf import _lib
+    sc, raw, _ = scene_and_raw(emu_lib, S.tiny)
+    full = asarf.FocusPlan(sc, lib=emu_lib).focus_host(raw)
+    plan = asarf.FocusPlan(sc, lib=emu_lib, keep_slc=False)
+    det = plan.focus_host(raw)
+    assert np.array_equal(det, full)
+    with pytest.raises(_lib.AsarfError):
+        plan.slc_into(np.zeros((4, 4), dtype=np.complex64))

@@ -156,3 +156,12 @@ def test_full_scene_matches_reference_build_given_its_doppler(gpu_lib):
     assert res["errors"] == 0
     assert out.shape == det.shape
     assert rel_rmse(out, det) < TOL_DETECTED
+
+
+@pytest.mark.parametrize("factory", [S.ers_small, asar_small])
+def test_detected_only_runs_equal_the_kept_slc_runs(gpu_lib, factory):
+    """keep_slc = 0 (the benchmark's detected product): bit-identical image."""
+    sc, raw, _ = scene_and_raw(gpu_lib, factory)
+    full = asarf.FocusPlan(sc, lib=gpu_lib).focus_host(raw)
+    det = asarf.FocusPlan(sc, lib=gpu_lib, keep_slc=False).focus_host(raw)
+    assert np.array_equal(det, full)
