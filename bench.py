@@ -250,8 +250,18 @@ def cpu_baseline_and_quality(sc_full, lib, forms: dict) -> tuple[dict, dict]:
     ref = rda.focus(raw, sc.to_dict())
     dt = time.perf_counter() - t0
     n = sc.range_size * lines
+    # the small ERS configuration in full (2048 x 4096), timed the same way
+    from asarf import scene as S
+    s0 = S.ers_small()
+    s0.prepare(lib)
+    raw0, _ = sim.simulate(s0, device="cuda")
+    t1 = time.perf_counter()
+    rda.focus(raw0, s0.to_dict())
+    dt0 = time.perf_counter() - t1
     base = {"value": round(n / dt / 1e6, 3), "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
             "cpu_model": _cpu_model(),
+            "ers_small_full": {"value": round(s0.range_size * s0.azimuth_size / dt0 / 1e6, 3), "unit": UNIT,
+                               "seconds": round(dt0, 2), "scene": "ERS-like 2048 x 4096, whole scene"},
             "sample": f"{sc.range_size} x {lines} scene with the workload's parameters and a 6x4 point grid "
                       f"({n / 1e6:.1f} Msamples) through the numpy FP64 oracle (scipy.fft workers=all cores), "
                       f"{dt:.1f} s"}
@@ -336,6 +346,73 @@ def _e2e_leg(args, sc, plan, lib, raw_np, opts, stream, st, world):
     blocking_ms = _max_over_ranks(b0.elapsed_time(b1) / 3, world)
     del plans[1:]
     return e2e_value, e2e_ms, blocking_ms, out_h
+
+
+def other_workloads(lib, steps: int, warmup: int) -> dict:
+    """The other configurations, measured in the same run so that the default bench line
+    carries them: the ASAR IM-like 5616 x 30000 8-bit scene, the same scene in FBAQ4 records,
+    the 16-segment uneven batch in one CUDA graph, and the 5616 x 120000 strip in overlapped
+    16384-line blocks; plain FP32, detected products, device-resident raw bytes, CUDA events
+    around `steps` runs after `warmup`."""
+    import torch
+    import asarf
+    from asarf import scene as S
+    from asarf import sim
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    out = {}
+    for name in ("asar_im", "asar_fbaq"):
+        sc = make_scene(name, 1002)
+        sc.prepare(lib)
+        raw = torch.from_numpy(sim.simulate(sc, device="cuda")[0]).cuda()
+        plan = asarf.FocusPlan(sc, lib=lib, keep_slc=False)
+        o = torch.empty(plan.out_shape, dtype=torch.float32, device="cuda")
+        ms = timed(lambda: plan.focus(raw, o, stream=st.cuda_stream))
+        if plan.results()["errors"]:
+            raise RuntimeError(f"{name} reported error flags")
+        out[name] = {"workload": _describe(sc), "ms_per_step": round(ms, 4),
+                     "value": round(sc.range_size * sc.azimuth_size / ms / 1e3, 1)}
+        plan.close()
+        del plan, raw, o
+    scenes = S.batch16()
+    for sc in scenes:
+        sc.prepare(lib)
+    raws = [torch.from_numpy(sim.simulate(sc, device="cuda")[0]).cuda() for sc in scenes]
+    batch = asarf.FocusBatch(scenes, lib=lib, options=[{"keep_slc": False}] * len(scenes))
+    outs = [torch.empty(p.out_shape, dtype=torch.float32, device="cuda") for p in batch.plans]
+    ms = timed(lambda: batch.focus(raws, outs, stream=st.cuda_stream))
+    n = sum(sc.range_size * sc.azimuth_size for sc in scenes)
+    out["batch16"] = {"workload": "16 uneven segments (ERS 5-bit / ASAR 8-bit, range 2048|5616, azimuth "
+                                  "U[4000, 30000]) in one CUDA graph", "ms_per_step": round(ms, 4),
+                      "value": round(n / ms / 1e3, 1)}
+    batch.close()
+    del batch, raws, outs
+    sc = make_scene("asar_strip", 1004)
+    sc.prepare(lib)
+    strip = asarf.FocusStrip(sc, block_lines=16384, overlap=1400, lib=lib)
+    raw = torch.from_numpy(sim.simulate(sc, device="cuda")[0]).cuda()
+    o = torch.empty(strip.out_shape, dtype=torch.float32, device="cuda")
+    ms = timed(lambda: strip.focus(raw, o, stream=st.cuda_stream))
+    if strip.errors():
+        raise RuntimeError("strip reported error flags")
+    out["asar_strip"] = {"workload": "ASAR-like 5616 x 120000 8-bit strip, Doppler drift +-100 Hz, 16384-line "
+                                     "blocks overlapping by 1400", "ms_per_step": round(ms, 4),
+                         "value": round(sc.range_size * sc.azimuth_size / ms / 1e3, 1)}
+    del strip, raw, o
+    torch.cuda.empty_cache()
+    return {"steps": steps, "warmup": warmup, "unit": UNIT, **out}
 
 
 def run_ours(args, rank: int, world: int, local: int) -> None:
@@ -487,6 +564,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "native_libs_mapped": _mapped_native_libs(),
         "clocks": clocks,
     }
+    if world == 1 and not args.no_workloads and args.workload == "ers_full":
+        line["other_workloads"] = other_workloads(lib, steps=5, warmup=3)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"], line["quality"] = cpu_baseline_and_quality(sc, lib, {"fp32": 0, "split": 1})
     print(json.dumps(line), flush=True)
@@ -771,6 +850,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API leg (profiling runs)")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other precision form")
     ap.add_argument("--no-tune", action="store_true", help="the planner's launch shapes, no timed autotuning")
+    ap.add_argument("--no-workloads", action="store_true", help="skip timing the other configurations")
     ap.add_argument("--precision", choices=["fp32", "split"], default="fp32",
                     help="azimuth transform form: plain FP32, or tensor-core bf16 hi+lo DFT tiles")
     args = ap.parse_args()
