@@ -56,7 +56,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     objdir.mkdir(exist_ok=True)
     common = ["-std=c++17", "-O3", "-lineinfo", f"-I{INC}", f"-I{CSRC}", "-Xcompiler", "-fPIC"]
     objs = []
-    for src in ("kernels.cu", "noalloc.cu", "host.cpp", "stages.cpp", "batch.cpp", "strip.cpp"):
+    for src in ("kernels.cu", "noalloc.cu", "host.cpp", "stages.cpp", "batch.cpp", "strip.cpp", "l0.cpp"):
         obj = objdir / (src + ".o")
         cmd = [NVCC, *GENCODE, *common, "-c", str(CSRC / src), "-o", str(obj)]
         if src.endswith(".cu") and verbose_ptxas:
@@ -80,7 +80,7 @@ def build_emu(out_dir: str | os.PathLike, force: bool = False) -> Path:
     cmd = [cxx, "-std=c++17", "-O2", "-ffp-contract=off", "-fno-strict-aliasing", "-fPIC", "-shared", "-DASARF_HOST_EMU",
            f"-I{INC}", f"-I{CSRC}", f"-I{CUDA_INC}", "-x", "c++", str(CSRC / "host.cpp"), "-x", "c++",
            str(CSRC / "stages.cpp"), "-x", "c++", str(CSRC / "batch.cpp"), "-x", "c++", str(CSRC / "strip.cpp"), "-x", "c++",
-           str(CSRC / "emu.cpp"),
+           str(CSRC / "l0.cpp"), "-x", "c++", str(CSRC / "emu.cpp"),
            "-o", str(out)]
     _run(cmd)
     return out

@@ -1207,6 +1207,30 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr, AzRdOut{&a, x0, k1});
 }
 
+// ----------------------------------------------------------------------------- ERS level-0 packets
+// Line y of an ERS IM measurement data set: its packet's 11232 measurement bytes go to raw
+// line y, its SWST and PRI codes (big-endian, ISP bytes 38-39 and 40-41 after the 32 bytes of
+// sensing time and FEP annotation) to swst[y] / pri[y]; the FEP ISP length (11465) and the
+// auxiliary section's 0xAA marker are checked as ParseErsLevel0ImPackets checks them
+// (envisat_format/src/ers_im_parse.cc:423-453).  Block y, threads over 2-byte words
+// (packet offsets are even: whole MDSRs of 11498 bytes).
+ASARF_HD ASARF_INLINE void ers_unpack_line(const ErsUnpackArgs& a, int y, int tid, int nthr) {
+    const uint8_t* pk = a.mdsr + ASARF_LDG(a.offset + y);
+    const uint16_t* src = reinterpret_cast<const uint16_t*>(pk + kErsMeasurementOffset);
+    uint16_t* dst = reinterpret_cast<uint16_t*>(a.raw + static_cast<long long>(y) * kErsMeasurementBytes);
+    for (int i = tid; i < kErsMeasurementBytes / 2; i += nthr) dst[i] = src[i];
+    if (tid == 0) {
+        const int isp_len = (pk[24] << 8) | pk[25];
+        unsigned e = 0;
+        if (isp_len != 11465) e |= kErrL0IspLength;
+        if (pk[32 + 4 + 10] != 0xAA) e |= kErrL0AuxMarker;
+        if (e) atomic_or_u32(a.errors, e);
+        const uint8_t* aux = pk + 32 + 4 + 10;  // 0xAA, OBRC/orbit, 4-byte OBT, activity, flags, 4-byte IF counter
+        if (a.swst) a.swst[y] = static_cast<uint16_t>((aux[12] << 8) | aux[13]);
+        if (a.pri) a.pri[y] = static_cast<uint16_t>((aux[14] << 8) | aux[15]);
+    }
+}
+
 // ----------------------------------------------------------------------------- L1 product records
 // Envisat MDS records of the level-1 products (ConditionResultsSLC / ConditionResultsDetected,
 // envisat_format/src/envisat_format_kernels.cu:28-114): `hdr` zero bytes of record header, then

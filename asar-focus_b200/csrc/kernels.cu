@@ -362,6 +362,10 @@ __global__ void __launch_bounds__(512) k_rc_rows(RcRowsArgs a) {
     rc_rows_body(a, blockIdx.x, threadIdx.x, blockDim.x, smem_rcr);
 }
 
+__global__ void __launch_bounds__(256) k_ers_unpack(ErsUnpackArgs a) {
+    ers_unpack_line(a, blockIdx.x, threadIdx.x, blockDim.x);
+}
+
 __global__ void __launch_bounds__(256) k_multilook(MultilookArgs a) {
     multilook_row_body(a, blockIdx.x, threadIdx.x, blockDim.x);
 }
@@ -561,6 +565,11 @@ int backend_rc_rows(const RcRowsArgs& a, int rows, LaunchShape sh, void* stream)
     if (rc) return rc;
     k_rc_rows<<<rows, sh.threads, sh.smem, S(stream)>>>(a);
     return check_launch("rc_rows");
+}
+int backend_ers_unpack(const ErsUnpackArgs& a, void* stream) {
+    if (a.lines <= 0) return ASARF_OK;
+    k_ers_unpack<<<a.lines, 256, 0, S(stream)>>>(a);
+    return check_launch("ers_unpack");
 }
 int backend_multilook(const MultilookArgs& a, void* stream) {
     k_multilook<<<a.out_y, 256, 0, S(stream)>>>(a);

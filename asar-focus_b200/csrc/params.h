@@ -273,6 +273,23 @@ struct DecodeArgs {
     long long stride;   // complex elements per image row
 };
 
+// ERS IM level-0 measurement data set (ERS_SAR_0P MDSRs of 11498 bytes) -> raw lines
+// (ParseErsLevel0ImPackets, envisat_format/src/ers_im_parse.cc:356-580)
+constexpr int kErsMdsrBytes = 11498;         // ers::highrate::MDSR_SIZE_BYTES
+constexpr int kErsMeasurementBytes = 11232;  // ers::highrate::MEASUREMENT_DATA_SIZE_BYTES (5616 I/Q pairs)
+constexpr int kErsMeasurementOffset = 266;   // 12 sensing time + 20 FEP + 4 record no. + 10 IDHT + 220 auxiliary
+constexpr unsigned kErrL0IspLength = 1u << 0;   // a packet's FEP ISP length is not 11465
+constexpr unsigned kErrL0AuxMarker = 1u << 1;   // a packet's auxiliary section does not start with 0xAA
+struct ErsUnpackArgs {
+    const uint8_t* mdsr;      // packets, in file order
+    const long long* offset;  // per line: byte offset of its packet in mdsr
+    int lines;
+    uint8_t* raw;             // [lines][kErsMeasurementBytes]
+    uint16_t* swst;           // per line SWST code (nullable)
+    uint16_t* pri;            // per line PRI code (nullable)
+    unsigned int* errors;     // kErrL0* bits
+};
+
 // ASAR FBAQ4 records -> complex rows, NaN where no sample (ConvertAsarImBlocksToComplex)
 struct DecodeFbaqArgs {
     const uint8_t* raw;

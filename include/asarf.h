@@ -259,6 +259,38 @@ int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_line_bytes, i
                                  int64_t total_raw_samples, int32_t stats_stride, double prf, asarf_raw_stats* d_out,
                                  void* stream);
 
+/* ---------------------------------------------------------------- ERS level-0 packets */
+
+/* ENVISAT-format time: days since 2000-01-01, seconds of the day, microseconds (mjd,
+ * envisat_format/include/envisat_types.h:37-72). */
+typedef struct asarf_mjd {
+    int32_t days;
+    uint32_t seconds;
+    uint32_t micros;
+} asarf_mjd;
+
+/* FetchErsL0ImForecastMeta (envisat_format/src/ers_im_parse.cc:228-354) over the measurement
+ * data set of an ERS_SAR_0P product held in host memory (`mdsr`, `blob_bytes` = num_dsr *
+ * dsr_size): the packet of each line (byte offset into mdsr) and its sensing time.  A packet
+ * whose data record number skips ahead is preceded by copies of the previous packet (at most
+ * 900, else ASARF_ERR_INVALID with the reference's message); packets before `start` / after
+ * `stop` are counted and trimmed to *packets_before_start / *packets_after_stop, which return
+ * the counts kept, as in the reference.  offsets / times (nullable) receive *count entries,
+ * `capacity` bounds them.  No PATC sensing-time correction is applied (the reference applies
+ * one only when a PATC auxiliary file is registered). */
+int asarf_ers_l0_forecast(const uint8_t* mdsr, int64_t blob_bytes, int64_t num_dsr, int64_t dsr_size,
+                          const asarf_mjd* start, const asarf_mjd* stop, int64_t* packets_before_start,
+                          int64_t* packets_after_stop, int64_t* offsets, asarf_mjd* times, int64_t capacity,
+                          int64_t* count);
+/* ParseErsLevel0ImPackets (envisat_format/src/ers_im_parse.cc:356-580) on the GPU: the packets
+ * as they lie in the file (d_mdsr, device memory, 2-byte aligned), one kernel for all `lines`:
+ * line y's 11232 measurement bytes -> d_raw + y * 11232 (the byte I/Q layout asarf_focus reads,
+ * raw_line_bytes = 11232), its SWST and PRI codes -> d_swst[y], d_pri[y] (nullable).  A packet
+ * whose FEP ISP length is not 11465 or whose auxiliary section does not start with 0xAA sets
+ * bit 0 / bit 1 of *d_errors (device memory, not cleared here).  Asynchronous on `stream`. */
+int asarf_ers_l0_unpack(const uint8_t* d_mdsr, const int64_t* d_offsets, int32_t lines, uint8_t* d_raw,
+                        uint16_t* d_swst, uint16_t* d_pri, uint32_t* d_errors, void* stream);
+
 /* ---------------------------------------------------------------- host FP64 geometry */
 
 /* InterpolateOrbit (sar/orbit_state_vector.cc:23-48). */
