@@ -665,14 +665,11 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         p->xt2 = opt.az_tile_width;
     }
     if (opt.precision == ASARF_PRECISION_SPLIT && opt.az_tile_width == 0) {
-        // the tensor-core transform converts R x wt operand rows in rounds of kSplitBlocks x 128:
-        // the widest even tile width (>= 32) that needs a single round, else the usual width
-        const int R = p->f2.plan.radix[p->f2.plan.nst - 1];
-        for (int xt = p->xt2; xt >= 32; xt -= 2)
-            if (R * (xt + p->hl + p->hr) <= kSplitBlocks * kSplitRows) {
-                p->xt2 = xt;
-                break;
-            }
+        // the split block holds the DFT matrix (16 KB) besides the tile: the widest tile that
+        // still leaves two blocks resident per SM
+        while (p->xt2 > 16 && az_rd_smem(p->n2, p->xt2 + p->hl + p->hr, p->xt2) + 2 * kSplitMatrixBytes >
+                                  kAzRdTwoBlockSmem)
+            p->xt2 -= 2;
     }
 
     // chirp matched filter in the forward transform's output order, scaled by 1/L
@@ -1036,8 +1033,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
         const int R = p->f2.plan.radix[p->f2.plan.nst - 1];
         const int m = p->n2 / R;
         const bool radix_ok = R == 2 || R == 3 || R == 4 || R == 5 || R == 7 || R == 8;
-        const size_t smem_split =
-            2 * static_cast<size_t>(kSplitBlocks) * kSplitOperandBytes + 2 * kSplitMatrixBytes + p->sh_rd.smem;
+        const size_t smem_split = 2 * static_cast<size_t>(kSplitMatrixBytes) + p->sh_rd.smem;
         if (p->use_tma && radix_ok && m >= 2 && 2 * m <= kSplitK && smem_split <= smem_optin_limit()) {
             std::vector<unsigned char> img;
             std::vector<float2> tws;

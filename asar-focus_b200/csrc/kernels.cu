@@ -182,64 +182,64 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
 // R * m, c < wt.  Operand row rho = r * wt + c holds the sub-sequence x[r + R mm] (mm < m) of
 // column c as bf16 hi + lo parts (K = (mm, re / im)); it multiplies the m-point DFT matrix B
 // (hi + lo, output slot s = frequency k1(s)) as Ahi Bhi + Ahi Blo + Alo Bhi with FP32
-// accumulation in TMEM, and the result times W_n2^(r k1(s)) goes back to row r + R s of column
-// c (a row of the same sub-sequence, already consumed).  Up to kSplitBlocks x 128 operand rows
-// are converted, multiplied and read back per round (one round for the tile widths the
-// planner picks where it can).  A radix-R FP32 pass over rows R s .. R s + R - 1 then leaves
-// frequency k1(s) + m k2 at row R s + k2: the digit-reversed order of the FP32 forward
-// transform (k1(s) is read from that transform's order table).
-// Returns false (error bit set, products drained) if a product did not complete in time.
-__device__ bool split_forward(const AzRdArgs& a, const AzRdSplit& sp, float2* s, unsigned char* a_hi,
-                              unsigned char* a_lo, const unsigned char* b_hi, const unsigned char* b_lo,
-                              uint32_t tmem, uint64_t* mbar, unsigned int* err) {
+// accumulation, and the result times W_n2^(r k1(s)) goes back to row r + R s of column c (a
+// row of the same sub-sequence, already consumed).  The operands live in tensor memory
+// beside the accumulator (TMEM columns [0, 64) accumulator, [64, 96) A hi, [96, 128) A lo),
+// so shared memory holds only B and the tile and two blocks stay resident per SM, as in the
+// FP32 kernel.  Rounds of 128 operand rows: warp w writes TMEM lanes 32 (w % 4) .., K chunk
+// w / 4 (8 inputs), one thread issues the products, every thread reads back its lane.  A
+// radix-R FP32 pass over rows R s .. R s + R - 1 then leaves frequency k1(s) + m k2 at row
+// R s + k2: the digit-reversed order of the FP32 forward transform (k1(s) from that
+// transform's order table).  Returns false (error bit set, products drained) if a product did
+// not complete in time.
+constexpr uint32_t kSplitColAcc = 0, kSplitColAHi = 64, kSplitColALo = 96;
+
+__device__ bool split_forward(const AzRdArgs& a, const AzRdSplit& sp, float2* s, const unsigned char* b_hi,
+                              const unsigned char* b_lo, uint32_t tmem, uint64_t* mbar, unsigned int* err) {
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int wt = a.wt, R = sp.radix, m = sp.m;
     const int rows = R * wt;
-    constexpr int kRound = kSplitBlocks * kSplitRows;
-    const int nkc = (m + 3) >> 2;  // chunks of 4 complex inputs holding data (the rest stay zero)
+    const int q = warp & 3, jb = warp >> 2;  // TMEM lane quarter, K chunk / accumulator column block
+    const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
     const FastDiv dwt = make_fastdiv(static_cast<unsigned int>(wt));
     constexpr uint32_t kIdesc = umma_idesc_bf16(kSplitRows, kSplitN);
     constexpr uint32_t kSbo = kSplitK * 16;  // 8 rows x K bf16
+    (void)nthr;
     uint32_t phase = 0;
-    for (int g0 = 0; g0 < rows; g0 += kRound) {
-        const int nrow = min(kRound, rows - g0);
-        const int nblk = (nrow + kSplitRows - 1) / kSplitRows;
-        for (int t = tid; t < nblk * kSplitRows * nkc; t += nthr) {
-            const int kc = t / (nblk * kSplitRows), rl = t - kc * (nblk * kSplitRows);
-            const int rho = g0 + rl;
-            uint32_t hi[4] = {0u, 0u, 0u, 0u}, lo[4] = {0u, 0u, 0u, 0u};
-            if (rl < nrow) {
-                const int r = static_cast<int>(fdiv_u(static_cast<unsigned int>(rho), dwt)), c = rho - r * wt;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int mm = 4 * kc + j;
-                    const float2 v = mm < m ? s[(r + R * mm) * wt + c] : make_float2(0.0f, 0.0f);
-                    split_bf16x2(v.x, v.y, hi[j], lo[j]);
-                }
-            }
-            const uint32_t off = static_cast<uint32_t>(kSplitOperandBytes) * (rl >> 7) + umma_offset(rl & 127, 8 * kc, kSplitK);
-            *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    for (int g0 = 0; g0 < rows; g0 += kSplitRows) {
+        const int rho = g0 + 32 * q + lane;
+        const bool live = rho < rows;
+        int r = 0, c = 0;
+        if (live) {
+            r = static_cast<int>(fdiv_u(static_cast<unsigned int>(rho), dwt));
+            c = rho - r * wt;
         }
-        fence_async_smem();
+        {
+            uint32_t hi[8], lo[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int mm = 8 * jb + i;
+                const float2 v = (live && mm < m) ? s[(r + R * mm) * wt + c] : make_float2(0.0f, 0.0f);
+                split_bf16x2(v.x, v.y, hi[i], lo[i]);
+            }
+            tmem_st8(tmem + lane_base + kSplitColAHi + 8u * jb, hi);
+            tmem_st8(tmem + lane_base + kSplitColALo + 8u * jb, lo);
+            tmem_wait_st();
+        }
         tc_fence_before_sync();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after_sync();
             const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
-            for (int b = 0; b < nblk; ++b) {
-                const uint32_t ah = smem_u32(a_hi) + kSplitOperandBytes * b, al = smem_u32(a_lo) + kSplitOperandBytes * b;
-                const uint32_t d = tmem + static_cast<uint32_t>(kSplitN) * b;
 #pragma unroll
-                for (int ks = 0; ks < kSplitK / 16; ++ks) {
-                    const uint32_t o = 256u * ks;  // two 128-byte core-matrix columns per k-step
-                    const uint64_t dah = umma_smem_desc(ah + o, 128, kSbo), dal = umma_smem_desc(al + o, 128, kSbo);
-                    const uint64_t dbh = umma_smem_desc(bh + o, 128, kSbo), dbl = umma_smem_desc(bl + o, 128, kSbo);
-                    umma_bf16(d, dah, dbh, kIdesc, ks > 0);
-                    umma_bf16(d, dah, dbl, kIdesc, true);
-                    umma_bf16(d, dal, dbh, kIdesc, true);
-                }
+            for (int ks = 0; ks < kSplitK / 16; ++ks) {
+                const uint32_t o = 256u * ks;  // B: two 128-byte core-matrix columns per k-step
+                const uint64_t dbh = umma_smem_desc(bh + o, 128, kSbo), dbl = umma_smem_desc(bl + o, 128, kSbo);
+                const uint32_t ah = tmem + kSplitColAHi + 8u * ks, al = tmem + kSplitColALo + 8u * ks;
+                umma_bf16_ts(tmem + kSplitColAcc, ah, dbh, kIdesc, ks > 0);
+                umma_bf16_ts(tmem + kSplitColAcc, ah, dbl, kIdesc, true);
+                umma_bf16_ts(tmem + kSplitColAcc, al, dbh, kIdesc, true);
             }
             umma_commit(mbar);
         }
@@ -251,25 +251,16 @@ __device__ bool split_forward(const AzRdArgs& a, const AzRdSplit& sp, float2* s,
         }
         phase ^= 1u;
         tc_fence_after_sync();
-        // accumulators: warp w reads TMEM lanes 32 (w % 4) .. and columns 16 (w / 4) .. (8 slots)
-        {
-            const int q = warp & 3, jb = warp >> 2;
-            if (8 * jb < m) {  // warp-uniform
-                for (int b = 0; b < nblk; ++b) {
-                    float v[16];
-                    tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + static_cast<uint32_t>(kSplitN * b + 16 * jb), v);
-                    const int rl = 128 * b + 32 * q + lane;
-                    if (rl < nrow) {
-                        const int rho = g0 + rl;
-                        const int r = static_cast<int>(fdiv_u(static_cast<unsigned int>(rho), dwt)), c = rho - r * wt;
+        // accumulator: this warp's lanes, columns 16 jb .. (output slots 8 jb ..)
+        if (8 * jb < m) {  // warp-uniform
+            float v[16];
+            tmem_ld16(tmem + lane_base + kSplitColAcc + 16u * jb, v);
+            if (live) {
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            const int slot = 8 * jb + i;
-                            if (slot < m)
-                                s[(r + R * slot) * wt + c] =
-                                    cmul(make_float2(v[2 * i], v[2 * i + 1]), __ldg(sp.tw + r * m + slot));
-                        }
-                    }
+                for (int i = 0; i < 8; ++i) {
+                    const int slot = 8 * jb + i;
+                    if (slot < m)
+                        s[(r + R * slot) * wt + c] = cmul(make_float2(v[2 * i], v[2 * i + 1]), __ldg(sp.tw + r * m + slot));
                 }
             }
         }
@@ -279,17 +270,16 @@ __device__ bool split_forward(const AzRdArgs& a, const AzRdSplit& sp, float2* s,
     // radix-R DFT over r of every (slot, column pair): rows R * slot + r, no twiddles
     const int npair = wt >> 1;
     fft_stage_pair_dispatch<false, false>(R, s, a.n2, 1, make_fastdiv(1u), npair,
-                                          make_fastdiv(static_cast<unsigned int>(npair)), wt, a.plan2.tw, tid, nthr);
+                                          make_fastdiv(static_cast<unsigned int>(npair)), wt, a.plan2.tw, tid,
+                                          blockDim.x);
     __syncthreads();
     return true;
 }
 
-__global__ void __launch_bounds__(512, 1) k_az_rd_split(AzRdArgs a, AzRdSplit sp, unsigned int* err,
+__global__ void __launch_bounds__(512, 2) k_az_rd_split(AzRdArgs a, AzRdSplit sp, unsigned int* err,
                                                         const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(1024) unsigned char smem_rds_raw[];
-    unsigned char* a_hi = smem_rds_raw;
-    unsigned char* a_lo = a_hi + kSplitBlocks * kSplitOperandBytes;
-    unsigned char* b_hi = a_lo + kSplitBlocks * kSplitOperandBytes;
+    unsigned char* b_hi = smem_rds_raw;
     unsigned char* b_lo = b_hi + kSplitMatrixBytes;
     float2* s = reinterpret_cast<float2*>(b_lo + kSplitMatrixBytes);
     const int wt = a.wt;
@@ -306,24 +296,18 @@ __global__ void __launch_bounds__(512, 1) k_az_rd_split(AzRdArgs a, AzRdSplit sp
         for (int r0 = 0; r0 < a.n2; r0 += a.n2_box)
             tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
     }
-    // while the tile is in flight: the DFT matrix images, zeros in the operand K chunks that
-    // never carry data (inputs >= m), the column / row tables
+    // the DFT matrix images and the column / row tables while the tile is in flight
     const uint4* bsrc = reinterpret_cast<const uint4*>(sp.bmat);
     for (int i = threadIdx.x; i < 2 * kSplitMatrixBytes / 16; i += blockDim.x)
         reinterpret_cast<uint4*>(b_hi)[i] = __ldg(bsrc + i);
-    {
-        const int nkc = (sp.m + 3) >> 2;
-        uint4* a0 = reinterpret_cast<uint4*>(a_hi);
-        for (int i = threadIdx.x; i < 2 * kSplitBlocks * kSplitOperandBytes / 16; i += blockDim.x)
-            if (((i >> 3) & 7) >= nkc) a0[i] = make_uint4(0u, 0u, 0u, 0u);
-    }
     az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbin);
+    fence_async_smem();  // B is read by the tensor cores
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
     const uint32_t tmem = tmem_base;
     mbar_wait(&bar, 0, err);
-    if (split_forward(a, sp, s, a_hi, a_lo, b_hi, b_lo, tmem, &mbar, err))
+    if (split_forward(a, sp, s, b_hi, b_lo, tmem, &mbar, err))
         az_rd_body<false>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, true);
     tc_fence_before_sync();
     __syncthreads();

@@ -184,10 +184,8 @@ struct AzRdArgs {
 constexpr int kSplitK = 64;          // K of the DFT tile: m <= 32 complex inputs as (re, im) pairs
 constexpr int kSplitN = 64;          // N: m <= 32 complex outputs as (re, im) pairs
 constexpr int kSplitRows = 128;      // M: range columns of the tile (wt <= 128)
-constexpr int kSplitOperandBytes = kSplitRows * kSplitK * 2;   // one bf16 A part (16 KB)
 constexpr int kSplitMatrixBytes = kSplitN * kSplitK * 2;       // one bf16 B part (8 KB)
-constexpr int kSplitBlocks = 3;      // operand row blocks per round (3 x 128 rows)
-constexpr int kSplitTmemCols = 256;  // kSplitBlocks accumulators of kSplitN columns, power of 2
+constexpr int kSplitTmemCols = 128;  // accumulator (64 columns) + A hi (32) + A lo (32), power of 2
 // Byte offset of element (row, k) of a 16-bit tensor-core operand with K elements per row in
 // the canonical no-swizzle K-major layout (8 x 8 core matrices of 128 contiguous bytes; K-adjacent
 // core matrices 128 bytes apart, row-adjacent groups 16 K bytes apart).

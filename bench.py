@@ -317,9 +317,9 @@ def _e2e_leg(args, sc, plan, lib, raw_np, opts, stream, st, world):
     for p_ in plans:
         if p_.results()["errors"]:
             raise RuntimeError("host run reported error flags")
-    # as many scenes as the timed device steps (at least 30): the pipeline's fill and drain
+    # as many scenes as the timed device steps (at least 100): the pipeline's fill and drain
     # (one scene's focusing and download) spread over the whole run
-    e2e_steps = max(30, args.steps)
+    e2e_steps = max(100, args.steps)
     _barrier(world)
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
@@ -513,7 +513,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                                                          stream, st, world)
         e2e = {"value": round(e2e_value, 1), "unit": UNIT,
                "h2d_bytes_per_step": int(raw_np.nbytes), "d2h_bytes_per_step": int(out_h[0].numel() * 4),
-               "ms_per_step": round(e2e_ms, 4), "steps": max(30, args.steps),
+               "ms_per_step": round(e2e_ms, 4), "steps": max(100, args.steps),
                "api": f"asarf_focus_host_async, scenes round-robin over {E2E_DEPTH} plans on their own "
                       f"streams, pinned host buffers (copies overlap focusing)",
                "blocking_ms_per_step": round(blocking_ms, 4),
