@@ -1,18 +1,19 @@
 // Fifth-generation tensor-core (tcgen05) helpers for sm_100a, in inline PTX.
 //
 // Used by the split-precision form of the azimuth transforms: small dense DFT tiles run as
-// bf16 x bf16 -> fp32 matrix products, A (data) and B (DFT matrix) staged in shared memory
-// in the canonical no-swizzle K-major layout, the accumulator D in tensor memory (TMEM).
-// One thread issues the products; completion is signalled through tcgen05.commit to a
+// bf16 x bf16 -> fp32 matrix products, A (data) in tensor memory (TMEM), B (DFT matrix) in
+// shared memory in the canonical no-swizzle K-major layout, the accumulator D in TMEM.  One
+// thread issues the products; completion is signalled through tcgen05.commit to a
 // shared-memory mbarrier whose waits are bounded (tma.cuh).
 //
-// Operand layout (no swizzle, K-major, 16-bit elements): a "core matrix" is 8 rows x 8
-// elements (16 bytes per row, 128 contiguous bytes).  Element (row, k) of an operand with
-// K elements per row lies at byte
+// Shared-memory operand layout (no swizzle, K-major, 16-bit elements): a "core matrix" is
+// 8 rows x 8 elements (16 bytes per row, 128 contiguous bytes).  Element (row, k) of an
+// operand with K elements per row lies at byte
 //     (row / 8) * SBO + (k / 8) * LBO + (row % 8) * 16 + (k % 8) * 2
-// with LBO = 128 (K-adjacent core matrices) and SBO = 128 * K / 8 (row-adjacent groups).
-// One kind::f16 product consumes K = 16, i.e. two core-matrix columns; the descriptor of
-// k-step s starts 2 * s * LBO bytes further.
+// with LBO = 128 (K-adjacent core matrices) and SBO = 128 * K / 8 (row-adjacent groups)
+// (umma_offset in params.h).  One kind::f16 product consumes K = 16, i.e. two core-matrix
+// columns; the descriptor of k-step s starts 2 * s * LBO bytes further.  In TMEM, row i of A
+// is lane i and K elements 2j, 2j + 1 share 32-bit column j (the lower index in the low half).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -65,16 +66,6 @@ __device__ __forceinline__ void tc_fence_after_sync() { asm volatile("tcgen05.fe
 
 // Generic-proxy shared-memory writes become visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-// D[taddr] (+)= A * B, one elected thread.
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                          bool accumulate) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.u32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
-        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate ? 1u : 0u)
-        : "memory");
-}
 
 // D[taddr] (+)= A * B with A in TMEM (lanes = rows, two 16-bit K elements per 32-bit column,
 // the lower K index in the low half) and B in shared memory, one elected thread.
