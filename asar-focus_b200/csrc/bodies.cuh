@@ -902,6 +902,9 @@ ASARF_HD ASARF_INLINE void store_pair(float2* dst, int x, int nk, float2 u, floa
     }
 }
 
+// R0, R1, R2, XT > 0: the transform's radix schedule and tile width as compile-time constants
+// (they must be the plan's: the planner picks this instantiation only when they are).
+template <int R0 = 0, int R1 = 0, int R2 = 0, int XT = 0>
 ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int b, int tid, int nthr, float2* s,
                                            const float2* tw, const int* rowmap, bool preloaded) {
     const int x0 = tile * a.xt;
@@ -926,7 +929,10 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
     if (!a.inverse) {
         // (writing the last stage straight to HBM, as the range-Doppler block does, measured
         // slower here: its rows scatter through the digit-reversed row map)
-        fft_forward_pairs<true, true>(a.plan1, s, xt, xt, tid, nthr);
+        if constexpr (R0 > 0)
+            fft_forward_pairs_ct3<R0, R1, R2, XT / 2, XT, true>(s, a.plan1.tw, tid, nthr);
+        else
+            fft_forward_pairs<true, true>(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
             const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
             const int x = x0 + c;
@@ -934,7 +940,10 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
         }
     } else {
         // conj(twiddle) of row k1 applied as the first stage loads the row
-        fft_inverse_dif_pairs<true, true>(a.plan1, s, xt, xt, tid, nthr, tw);
+        if constexpr (R0 > 0)
+            fft_inverse_dif_pairs_ct3<R0, R1, R2, XT / 2, XT, true>(s, a.plan1.tw, tid, nthr, tw);
+        else
+            fft_inverse_dif_pairs<true, true>(a.plan1, s, xt, xt, tid, nthr, tw);
         const int lo = a.state ? a.state->first_line : 0;
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {

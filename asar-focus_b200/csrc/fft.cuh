@@ -445,8 +445,42 @@ ASARF_HD ASARF_INLINE void pair_twiddle(float2* u, float2* v, float2 w1) {
     }
 }
 
+// One butterfly of a column-pair stage: block b, offset j (M = S * R), column pair cp.
 // PRE: the loaded values of row l are first multiplied by conj(pre[l]) (a per-row table, here the
 // input twiddles of the inverse strided pass), saving a separate pass over the tile.
+template <int R, bool INV, bool TW_FIRST, bool PRE, class Epi, bool PTW>
+ASARF_HD ASARF_INLINE void pair_item(float2* s, int b, int j, int cp, int M, int S, int ldc, int tw_step,
+                                     const float2* __restrict__ tw, const float2* pre, const Epi& epi) {
+    const int st = (S * ldc) >> 1;  // float4 units
+    float4* p = reinterpret_cast<float4*>(s + (b * M + j) * ldc) + cp;
+    float2 u[R], v[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        const float4 q = p[m * st];
+        u[m] = make_float2(q.x, q.y);
+        v[m] = make_float2(q.z, q.w);
+        if constexpr (PRE) {
+            const float2 w = pre[b * M + j + m * S];
+            u[m] = cmulc(u[m], w);
+            v[m] = cmulc(v[m], w);
+        }
+    }
+    // W_M^{j q}: one table load, higher powers by recurrence (error ~ q ulp); a table load
+    // per q is exact but measured slower
+    const float2 w1 = j != 0 ? ASARF_LDG(tw + j * tw_step) : make_float2(1.0f, 0.0f);
+    if (TW_FIRST && j != 0) pair_twiddle<R, INV, PTW>(u, v, w1);
+    dft_any<R, INV>(u);
+    dft_any<R, INV>(v);
+    if (!TW_FIRST && j != 0) pair_twiddle<R, INV, PTW>(u, v, w1);
+    if constexpr (Epi::kActive) {
+#pragma unroll
+        for (int m = 0; m < R; ++m) epi(b * M + j + m * S, cp, u[m], v[m]);
+    } else {
+#pragma unroll
+        for (int m = 0; m < R; ++m) p[m * st] = make_float4(u[m].x, u[m].y, v[m].x, v[m].y);
+    }
+}
+
 template <int R, bool INV, bool TW_FIRST, bool PRE = false, class Epi = NoEpi, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv& sdiv, int npair, const FastDiv& pdiv,
                                           int ldc, const float2* __restrict__ tw, int tid, int nthr,
@@ -454,39 +488,30 @@ ASARF_HD ASARF_INLINE void fft_stage_pair(float2* s, int n, int S, const FastDiv
     const int M = S * R;
     const int items = (n / R) * npair;
     const int tw_step = n / M;
-    const int st = (S * ldc) >> 1;  // float4 units
     for (int t = tid; t < items; t += nthr) {
         const int bj = static_cast<int>(fdiv_u(t, pdiv));
         const int cp = t - bj * npair;
         const int b = static_cast<int>(fdiv_u(bj, sdiv));
         const int j = bj - b * S;
-        float4* p = reinterpret_cast<float4*>(s + (b * M + j) * ldc) + cp;
-        float2 u[R], v[R];
-#pragma unroll
-        for (int m = 0; m < R; ++m) {
-            const float4 q = p[m * st];
-            u[m] = make_float2(q.x, q.y);
-            v[m] = make_float2(q.z, q.w);
-            if constexpr (PRE) {
-                const float2 w = pre[b * M + j + m * S];
-                u[m] = cmulc(u[m], w);
-                v[m] = cmulc(v[m], w);
-            }
-        }
-        // W_M^{j q}: one table load, higher powers by recurrence (error ~ q ulp); a table load
-        // per q is exact but measured slower
-        const float2 w1 = j != 0 ? ASARF_LDG(tw + j * tw_step) : make_float2(1.0f, 0.0f);
-        if (TW_FIRST && j != 0) pair_twiddle<R, INV, PTW>(u, v, w1);
-        dft_any<R, INV>(u);
-        dft_any<R, INV>(v);
-        if (!TW_FIRST && j != 0) pair_twiddle<R, INV, PTW>(u, v, w1);
-        if constexpr (Epi::kActive) {
-#pragma unroll
-            for (int m = 0; m < R; ++m) epi(b * M + j + m * S, cp, u[m], v[m]);
-        } else {
-#pragma unroll
-            for (int m = 0; m < R; ++m) p[m * st] = make_float4(u[m].x, u[m].y, v[m].x, v[m].y);
-        }
+        pair_item<R, INV, TW_FIRST, PRE, Epi, PTW>(s, b, j, cp, M, S, ldc, tw_step, tw, pre, epi);
+    }
+}
+
+// The same stage with every size a compile-time constant (length N, span S, NPAIR column pairs
+// of row stride LDC): the index arithmetic folds into constant multiplies and shifts.
+template <int R, bool INV, bool TW_FIRST, int N, int S, int NPAIR, int LDC, bool PRE = false, class Epi = NoEpi,
+          bool PTW = false>
+ASARF_HD ASARF_INLINE void fft_stage_pair_ct(float2* s, const float2* __restrict__ tw, int tid, int nthr,
+                                             const float2* pre = nullptr, const Epi& epi = Epi()) {
+    constexpr int M = S * R;
+    constexpr int ITEMS = (N / R) * NPAIR;
+    constexpr int TW_STEP = N / M;
+    for (int t = tid; t < ITEMS; t += nthr) {
+        const int bj = t / NPAIR;
+        const int cp = t - bj * NPAIR;
+        const int b = bj / S;
+        const int j = bj - b * S;
+        pair_item<R, INV, TW_FIRST, PRE, Epi, PTW>(s, b, j, cp, M, S, LDC, TW_STEP, tw, pre, epi);
     }
 }
 
@@ -566,6 +591,33 @@ ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs(const FftPlan& p, float2* s, in
                                                                          npair, pdiv, ldc, p.tw, tid, nthr);
         ASARF_SYNC();
     }
+}
+
+// Compile-time three-stage column-pair transforms (radices R0, R1, R2 first stage first, NPAIR
+// column pairs of row stride LDC): the forward DIF and the inverse in DIF form of the strided
+// azimuth pass, with the same stage sequence, twiddle tables and rounding as the run-time
+// versions above (fft_forward_pairs / fft_inverse_dif_pairs), so the results are identical.
+template <int R0, int R1, int R2, int NPAIR, int LDC, bool PTW>
+ASARF_HD ASARF_INLINE void fft_forward_pairs_ct3(float2* s, const float2* __restrict__ tw, int tid, int nthr) {
+    constexpr int N = R0 * R1 * R2;
+    fft_stage_pair_ct<R0, false, false, N, N / R0, NPAIR, LDC, false, NoEpi, PTW>(s, tw, tid, nthr);
+    ASARF_SYNC();
+    fft_stage_pair_ct<R1, false, false, N, N / (R0 * R1), NPAIR, LDC, false, NoEpi, PTW>(s, tw, tid, nthr);
+    ASARF_SYNC();
+    fft_stage_pair_ct<R2, false, false, N, 1, NPAIR, LDC, false, NoEpi, PTW>(s, tw, tid, nthr);
+    ASARF_SYNC();
+}
+
+template <int R0, int R1, int R2, int NPAIR, int LDC, bool PTW>
+ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs_ct3(float2* s, const float2* __restrict__ tw, int tid, int nthr,
+                                                     const float2* pre) {
+    constexpr int N = R0 * R1 * R2;
+    fft_stage_pair_ct<R0, true, false, N, N / R0, NPAIR, LDC, true, NoEpi, PTW>(s, tw, tid, nthr, pre);
+    ASARF_SYNC();
+    fft_stage_pair_ct<R1, true, false, N, N / (R0 * R1), NPAIR, LDC, false, NoEpi, PTW>(s, tw, tid, nthr);
+    ASARF_SYNC();
+    fft_stage_pair_ct<R2, true, false, N, 1, NPAIR, LDC, false, NoEpi, PTW>(s, tw, tid, nthr);
+    ASARF_SYNC();
 }
 
 template <bool INV>

@@ -135,6 +135,8 @@ __global__ void __launch_bounds__(CtSchedule<L>::nthr, 2) k_range_compress_ct(Ra
 }
 
 // Strided azimuth pass: the [n1][xt] tile (rows r*n2 + b) arrives by 3-D TMA boxes.
+// R0..XT > 0: compile-time transform schedule and tile width (az_strided_body).
+template <int R0 = 0, int R1 = 0, int R2 = 0, int XT = 0>
 __global__ void __launch_bounds__(512) k_az_strided(AzStridedArgs a, const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(1024) unsigned char smem_as_raw[];
     float2* s = reinterpret_cast<float2*>(smem_as_raw);
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(512) k_az_strided(AzStridedArgs a, const __gri
     az_strided_tables(a, blockIdx.y, threadIdx.x, blockDim.x, tw, row);
     __syncthreads();
     if (a.use_tma) mbar_wait(&bar, 0, a.state ? &const_cast<FocusState*>(a.state)->errors : nullptr);
-    az_strided_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, tw, row, a.use_tma != 0);
+    az_strided_body<R0, R1, R2, XT>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, tw, row, a.use_tma != 0);
 }
 
 // Range-Doppler block: the [n2][wt] tile (contiguous rows, range halo) arrives by 2-D TMA
@@ -449,11 +451,26 @@ static CUtensorMap tmap_or_zero(const void* tmap) {
     return m;
 }
 
-int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream) {
-    int rc = ensure_smem(k_az_strided, sh.smem, "az_strided");
+template <int R0, int R1, int R2, int XT>
+static int launch_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh,
+                             void* stream) {
+    int rc = ensure_smem(k_az_strided<R0, R1, R2, XT>, sh.smem, "az_strided");
     if (rc) return rc;
-    k_az_strided<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, tmap_or_zero(tmap));
+    k_az_strided<R0, R1, R2, XT><<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, tmap_or_zero(tmap));
     return check_launch("az_strided");
+}
+
+// Compile-time instantiations for the strided lengths of the ERS-like (225 = 9 x 5 x 5) and
+// ASAR IM-like (180 = 9 x 4 x 5) scenes at the 32-column tile; every other plan runs the
+// run-time schedule.
+static bool plan_is(const FftPlan& p, int r0, int r1, int r2) {
+    return p.nst == 3 && p.radix[0] == r0 && p.radix[1] == r1 && p.radix[2] == r2;
+}
+
+int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream) {
+    if (a.xt == 32 && plan_is(a.plan1, 9, 5, 5)) return launch_az_strided<9, 5, 5, 32>(a, tmap, tiles, nblocks, sh, stream);
+    if (a.xt == 32 && plan_is(a.plan1, 9, 4, 5)) return launch_az_strided<9, 4, 5, 32>(a, tmap, tiles, nblocks, sh, stream);
+    return launch_az_strided<0, 0, 0, 0>(a, tmap, tiles, nblocks, sh, stream);
 }
 
 int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, unsigned int* err,
