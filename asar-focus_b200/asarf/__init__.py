@@ -45,7 +45,7 @@ class FocusPlan:
                  lib_path=None, dc_poly=None, product: int = 0, calibration: float = 1.0,
                  record_header_bytes: int = 17, sq_stats: bool = False, precision: int = 0,
                  absolute_phase: bool = False, az_n2: int = 0, az_tile_width: int = 0, strided_tile_width: int = 0,
-                 keep_slc: bool = True):
+                 keep_slc: bool = True, compiled_schedules: bool = True):
         self.lib = lib or load_library(lib_path)
         self.scene = scene
         if scene.vr_poly is None or not scene.osv:
@@ -68,6 +68,7 @@ class FocusPlan:
         opt.az_tile_width = int(az_tile_width)
         opt.strided_tile_width = int(strided_tile_width)
         opt.keep_slc = int(bool(keep_slc))
+        opt.compiled_schedules = int(bool(compiled_schedules))
         self.product = int(product)
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_plan_create(C.byref(self._sc), C.byref(opt), C.byref(h)), "plan_create")
@@ -217,7 +218,8 @@ class FocusBatch:
             opts[i].ref_compat_stats = int(bool(ref_compat_stats))
             opts[i].precision = int(precision)
             for k, v in ((options[i] if options else None) or {}).items():
-                if k in ("az_n2", "az_tile_width", "strided_tile_width", "rc_fft_len", "precision", "keep_slc"):
+                if k in ("az_n2", "az_tile_width", "strided_tile_width", "rc_fft_len", "precision", "keep_slc",
+                         "compiled_schedules"):
                     setattr(opts[i], k, int(v))
         h = C.c_void_p()
         _lib.check(self.lib, self.lib.asarf_batch_create(arr, n, C.cast(opts, C.c_void_p), int(branches), C.byref(h)),

@@ -39,7 +39,8 @@ class Options(C.Structure):
                 ("dc_poly_given", C.c_int32), ("dc_poly", C.c_double * 3), ("product", C.c_int32),
                 ("record_header_bytes", C.c_int32), ("calibration", C.c_float), ("sq_stats", C.c_int32),
                 ("precision", C.c_int32), ("absolute_phase", C.c_int32), ("az_n2", C.c_int32),
-                ("az_tile_width", C.c_int32), ("strided_tile_width", C.c_int32), ("keep_slc", C.c_int32)]
+                ("az_tile_width", C.c_int32), ("strided_tile_width", C.c_int32), ("keep_slc", C.c_int32),
+                ("compiled_schedules", C.c_int32)]
 
 
 PRECISION_FP32 = 0
@@ -57,7 +58,7 @@ class Dims(C.Structure):
         ("out_cols", C.c_int32 * 2), ("out_rows_max", C.c_int32), ("out_cols_max", C.c_int32),
         ("max_aperture", C.c_int32), ("vr_poly", C.c_double * 3), ("device_bytes", C.c_size_t),
         ("out_bytes_max", C.c_int64), ("precision", C.c_int32), ("split_radix", C.c_int32), ("split_m", C.c_int32),
-        ("az_tile_width", C.c_int32), ("strided_tile_width", C.c_int32),
+        ("az_tile_width", C.c_int32), ("strided_tile_width", C.c_int32), ("compiled_schedules", C.c_int32),
     ]
 
 

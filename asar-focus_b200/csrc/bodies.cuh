@@ -1150,8 +1150,9 @@ struct AzRdOut {
 };
 
 // FWD = false: the caller has already put the tile through the forward transform (the
-// split-precision kernel's tensor-core DFT) and synchronised.
-template <bool FWD = true>
+// split-precision kernel's tensor-core DFT) and synchronised.  R0, R1, R2 > 0: the n2
+// transforms' radix schedule as compile-time constants (it must be the plan's).
+template <bool FWD = true, int R0 = 0, int R1 = 0, int R2 = 0>
 ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s,
                                       const ColParams* cps, const int* fbin, unsigned int* err_flag, bool preloaded) {
     const int x0 = tile * a.xt;
@@ -1168,7 +1169,10 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     }
     if constexpr (FWD) {
         ASARF_SYNC();
-        fft_forward_pairs(a.plan2, s, wt, wt, tid, nthr);
+        if constexpr (R0 > 0)
+            fft_forward_pairs_cs3<R0, R1, R2>(s, wt, wt, a.plan2.tw, tid, nthr);
+        else
+            fft_forward_pairs(a.plan2, s, wt, wt, tid, nthr);
     }
     // RCMC + matched filter.  Every output (row p, column c) reads taps of row p only, so a
     // row is computed into registers by one warp (lane = column, xt <= 64), the warp
@@ -1213,7 +1217,10 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     }
 #endif
     // the inverse transform's last stage stores the block's rows k1 * n2 + r directly
-    fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr, AzRdOut{&a, x0, k1});
+    if constexpr (R0 > 0)
+        fft_inverse_pairs_cs3<R0, R1, R2>(s + a.hl, a.xt, wt, a.plan2.tw, tid, nthr, AzRdOut{&a, x0, k1});
+    else
+        fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr, AzRdOut{&a, x0, k1});
 }
 
 // ----------------------------------------------------------------------------- ERS level-0 packets

@@ -515,6 +515,24 @@ ASARF_HD ASARF_INLINE void fft_stage_pair_ct(float2* s, const float2* __restrict
     }
 }
 
+// The same stage with the length N and span S compile-time constants and the column count
+// run-time (npair pairs, divider pdiv, row stride ldc): the range-Doppler block, whose tile
+// width follows the scene's range walk.
+template <int R, bool INV, bool TW_FIRST, int N, int S, class Epi = NoEpi>
+ASARF_HD ASARF_INLINE void fft_stage_pair_cs(float2* s, int npair, const FastDiv& pdiv, int ldc,
+                                             const float2* __restrict__ tw, int tid, int nthr,
+                                             const Epi& epi = Epi()) {
+    constexpr int M = S * R;
+    const int items = (N / R) * npair;
+    for (int t = tid; t < items; t += nthr) {
+        const int bj = static_cast<int>(fdiv_u(t, pdiv));
+        const int cp = t - bj * npair;
+        const int b = bj / S;
+        const int j = bj - b * S;
+        pair_item<R, INV, TW_FIRST, false, Epi, false>(s, b, j, cp, M, S, ldc, N / M, tw, nullptr, epi);
+    }
+}
+
 // Column-pair stages take the prime-power radices: a larger composite radix holds twice its
 // length in registers per column pair, which lifts the azimuth kernels from 64 to 128
 // registers per thread and halves their resident CTAs (measured slower despite fewer passes).
@@ -617,6 +635,37 @@ ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs_ct3(float2* s, const float2* __
     fft_stage_pair_ct<R1, true, false, N, N / (R0 * R1), NPAIR, LDC, false, NoEpi, PTW>(s, tw, tid, nthr);
     ASARF_SYNC();
     fft_stage_pair_ct<R2, true, false, N, 1, NPAIR, LDC, false, NoEpi, PTW>(s, tw, tid, nthr);
+    ASARF_SYNC();
+}
+
+// Three-stage forward DIF (fft_forward_pairs) and inverse DIT with epilogue (fft_inverse_pairs)
+// of a compile-time radix schedule R0, R1, R2 over a run-time number of columns: the same
+// stages, twiddles and rounding as the run-time versions.
+template <int R0, int R1, int R2>
+ASARF_HD ASARF_INLINE void fft_forward_pairs_cs3(float2* s, int ncol, int ldc, const float2* __restrict__ tw, int tid,
+                                                 int nthr) {
+    constexpr int N = R0 * R1 * R2;
+    const int npair = ncol >> 1;
+    const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
+    fft_stage_pair_cs<R0, false, false, N, N / R0>(s, npair, pdiv, ldc, tw, tid, nthr);
+    ASARF_SYNC();
+    fft_stage_pair_cs<R1, false, false, N, R2>(s, npair, pdiv, ldc, tw, tid, nthr);
+    ASARF_SYNC();
+    fft_stage_pair_cs<R2, false, false, N, 1>(s, npair, pdiv, ldc, tw, tid, nthr);
+    ASARF_SYNC();
+}
+
+template <int R0, int R1, int R2, class Epi = NoEpi>
+ASARF_HD ASARF_INLINE void fft_inverse_pairs_cs3(float2* s, int ncol, int ldc, const float2* __restrict__ tw, int tid,
+                                                 int nthr, const Epi& epi = Epi()) {
+    constexpr int N = R0 * R1 * R2;
+    const int npair = ncol >> 1;
+    const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
+    fft_stage_pair_cs<R2, true, true, N, 1>(s, npair, pdiv, ldc, tw, tid, nthr);
+    ASARF_SYNC();
+    fft_stage_pair_cs<R1, true, true, N, R2>(s, npair, pdiv, ldc, tw, tid, nthr);
+    ASARF_SYNC();
+    fft_stage_pair_cs<R0, true, true, N, N / R0, Epi>(s, npair, pdiv, ldc, tw, tid, nthr, epi);
     ASARF_SYNC();
 }
 

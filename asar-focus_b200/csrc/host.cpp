@@ -464,6 +464,7 @@ void asarf_default_options(asarf_options* opt) {
     opt->az_tile_width = 0;
     opt->strided_tile_width = 0;
     opt->keep_slc = 1;
+    opt->compiled_schedules = 1;
 }
 
 int32_t asarf_fft_size_above(int32_t v) { return fft_size_above(v); }
@@ -953,6 +954,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     d.state = p->state;
     d.win = win;
     d.absolute_phase = opt.absolute_phase ? 1 : 0;
+    d.compiled = p->a_fwd.compiled = p->a_inv.compiled = opt.compiled_schedules ? 1 : 0;
     d.lambda_d = s.wavelength;
     p->tiles2 = (p->nk + p->xt2 - 1) / p->xt2;
     p->sh_rd = {512, az_rd_smem(p->n2, d.wt, d.xt)};
@@ -1090,6 +1092,8 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     dm.split_m = p->split ? p->a_split.m : 0;
     dm.az_tile_width = p->xt2;
     dm.strided_tile_width = p->xt1;
+    dm.compiled_schedules = (p->a_fwd.compiled && strided_schedule_compiled(p->a_fwd.plan1, p->a_fwd.xt) ? 1 : 0) |
+                            (p->a_rd.compiled && block_schedule_compiled(p->a_rd.plan2) ? 2 : 0);
     *out = p;
     return ASARF_OK;
 }

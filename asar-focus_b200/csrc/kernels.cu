@@ -158,6 +158,8 @@ __global__ void __launch_bounds__(512) k_az_strided(AzStridedArgs a, const __gri
 
 // Range-Doppler block: the [n2][wt] tile (contiguous rows, range halo) arrives by 2-D TMA
 // boxes; columns left of 0 and right of nk are filled with zeros by the TMA unit.
+// R0..R2 > 0: compile-time radix schedule of the n2 transforms (az_rd_body).
+template <int R0 = 0, int R1 = 0, int R2 = 0>
 __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(1024) unsigned char smem_rd_raw[];
     const int wt = a.wt;
@@ -176,7 +178,8 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
     az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbin);
     __syncthreads();
     if (a.use_tma) mbar_wait(&bar, 0, err);
-    az_rd_body(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, a.use_tma != 0);
+    az_rd_body<true, R0, R1, R2>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err,
+                                 a.use_tma != 0);
 }
 
 // ----------------------------------------------------------------------------- split precision
@@ -460,25 +463,32 @@ static int launch_az_strided(const AzStridedArgs& a, const void* tmap, int tiles
     return check_launch("az_strided");
 }
 
-// Compile-time instantiations for the strided lengths of the ERS-like (225 = 9 x 5 x 5) and
-// ASAR IM-like (180 = 9 x 4 x 5) scenes at the 32-column tile; every other plan runs the
-// run-time schedule.
-static bool plan_is(const FftPlan& p, int r0, int r1, int r2) {
-    return p.nst == 3 && p.radix[0] == r0 && p.radix[1] == r1 && p.radix[2] == r2;
-}
-
+// The compiled schedules (strided_schedule_compiled) when the plan allows them.
 int backend_az_strided(const AzStridedArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, void* stream) {
-    if (a.xt == 32 && plan_is(a.plan1, 9, 5, 5)) return launch_az_strided<9, 5, 5, 32>(a, tmap, tiles, nblocks, sh, stream);
-    if (a.xt == 32 && plan_is(a.plan1, 9, 4, 5)) return launch_az_strided<9, 4, 5, 32>(a, tmap, tiles, nblocks, sh, stream);
+    if (a.compiled && strided_schedule_compiled(a.plan1, a.xt)) {
+        if (plan_is(a.plan1, 9, 5, 5)) return launch_az_strided<9, 5, 5, 32>(a, tmap, tiles, nblocks, sh, stream);
+        return launch_az_strided<9, 4, 5, 32>(a, tmap, tiles, nblocks, sh, stream);
+    }
     return launch_az_strided<0, 0, 0, 0>(a, tmap, tiles, nblocks, sh, stream);
 }
 
+template <int R0, int R1, int R2>
+static int launch_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh,
+                        unsigned int* err, void* stream) {
+    int rc = ensure_smem(k_az_rd<R0, R1, R2>, sh.smem, "az_rd");
+    if (rc) return rc;
+    k_az_rd<R0, R1, R2><<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, err, tmap_or_zero(tmap));
+    return check_launch("az_rd");
+}
+
+// The compiled schedules (block_schedule_compiled) when the plan allows them.
 int backend_az_rd(const AzRdArgs& a, const void* tmap, int tiles, int nblocks, LaunchShape sh, unsigned int* err,
                   void* stream) {
-    int rc = ensure_smem(k_az_rd, sh.smem, "az_rd");
-    if (rc) return rc;
-    k_az_rd<<<dim3(tiles, nblocks), sh.threads, sh.smem, S(stream)>>>(a, err, tmap_or_zero(tmap));
-    return check_launch("az_rd");
+    if (a.compiled && block_schedule_compiled(a.plan2)) {
+        if (plan_is(a.plan2, 5, 5, 5)) return launch_az_rd<5, 5, 5>(a, tmap, tiles, nblocks, sh, err, stream);
+        return launch_az_rd<8, 7, 3>(a, tmap, tiles, nblocks, sh, err, stream);
+    }
+    return launch_az_rd<0, 0, 0>(a, tmap, tiles, nblocks, sh, err, stream);
 }
 
 int backend_az_rd_split(const AzRdArgs& a, const AzRdSplit& sp, const void* tmap, int tiles, int nblocks,

@@ -127,6 +127,18 @@ struct RangeCompressArgs {
     const float* lut_q;
 };
 
+// Transform schedules with compile-time instantiations of the azimuth kernels (the strided
+// lengths 225 = 9 x 5 x 5 and 180 = 9 x 4 x 5 at the 32-column tile, the block lengths
+// 125 = 5 x 5 x 5 and 168 = 8 x 7 x 3 of the ERS-like and ASAR IM-like scenes); every other
+// schedule runs the run-time loops, with the same arithmetic.
+ASARF_HD inline bool plan_is(const FftPlan& p, int r0, int r1, int r2) {
+    return p.nst == 3 && p.radix[0] == r0 && p.radix[1] == r1 && p.radix[2] == r2;
+}
+ASARF_HD inline bool strided_schedule_compiled(const FftPlan& p, int xt) {
+    return xt == 32 && (plan_is(p, 9, 5, 5) || plan_is(p, 9, 4, 5));
+}
+ASARF_HD inline bool block_schedule_compiled(const FftPlan& p) { return plan_is(p, 5, 5, 5) || plan_is(p, 8, 7, 3); }
+
 struct AzStridedArgs {
     const float2* in;
     float2* out;
@@ -146,6 +158,7 @@ struct AzStridedArgs {
     int out_row0;         // inverse: row r is stored at out + (r - out_row0) * pitch
     float* out_intensity; // inverse: when set, |z|^2 of row r goes to out_intensity + (r - out_row0) * pitch
                           // (floats) and no complex row is stored
+    int compiled;         // 1: launch a compile-time instantiation of plan1's schedule when one exists
 };
 
 // Per range column constants of the range-Doppler block.
@@ -177,6 +190,7 @@ struct AzRdArgs {
     int n2_box;           // rows per TMA box
     int absolute_phase;   // 1: multiply column x by exp(j (4 pi R0 / lambda + pi dc_off^2 / Ka)) (FP64)
     double lambda_d;      // wavelength, FP64
+    int compiled;         // 1: launch a compile-time instantiation of plan2's schedule when one exists
 };
 
 // Split-precision form of the range-Doppler block's forward transform: n2 = radix * m,

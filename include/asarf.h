@@ -115,6 +115,10 @@ typedef struct asarf_options {
                                   (asarf_plan_slc, IMS records, the IMP product statistics);
                                   0: detected output only -- the inverse azimuth pass writes |z|^2 rows
                                   (half the bytes written, and read again by the multilook) */
+    int32_t compiled_schedules; /* 1 (default): azimuth transforms whose radix schedule has a compile-time
+                                  instantiation (strided 225 = 9*5*5 and 180 = 9*4*5 at 32 columns,
+                                  blocks 125 = 5*5*5 and 168 = 8*7*3) run it; 0: run-time schedules only.
+                                  Both give identical results */
 } asarf_options;
 
 /* Arithmetic of the azimuth transforms (asarf_options.precision).  The reference runs every
@@ -141,6 +145,8 @@ typedef struct asarf_dims {
     int32_t precision;         /* ASARF_PRECISION_* the plan runs (SPLIT falls back to FP32 where n2 does not split) */
     int32_t split_radix, split_m; /* with SPLIT: n2 = split_radix * split_m */
     int32_t az_tile_width, strided_tile_width; /* launch shapes in use */
+    int32_t compiled_schedules; /* bit 0: the strided passes, bit 1: the range-Doppler block run a
+                                   compile-time schedule */
 } asarf_dims;
 
 /* Per-run results: SARResults (sar/sar_metadata.h:46-55) plus the chosen window. */

@@ -8,6 +8,8 @@
 * ASAR IM-like 5616 x 30000 (8-bit I/Q, quadratic Doppler): the same against the oracle with
   data-only statistics (the other statistics mode), and against the reference build.
 
+* Both: the compile-time transform schedules against the run-time ones, bit for bit.
+
 The oracle runs once per scene (about a minute on the host cores) and is shared by the
 tests of that scene.
 """
@@ -129,3 +131,21 @@ def test_ers_full_scene_own_doppler_matches_reference_build(gpu_lib):
 
 def test_asar_full_scene_matches_reference_build(gpu_lib):
     _check_against_reference_build(gpu_lib, S.asar_im, max_bad_cols=64)
+
+
+@pytest.mark.parametrize("factory", [S.ers_full, S.asar_im])
+def test_compiled_schedules_equal_run_time_schedules(gpu_lib, factory):
+    """The compile-time instantiations of the azimuth transforms (strided 225 / 180, blocks 125
+    / 168: both full scenes take both) run the run-time schedules' operations in the same order:
+    image and SLC bit-identical with them switched off."""
+    sc, raw, _ = scene_and_raw(gpu_lib, factory, device="cuda")
+    runs = []
+    for compiled in (True, False):
+        plan = asarf.FocusPlan(sc, lib=gpu_lib, compiled_schedules=compiled)
+        assert plan.dims["compiled_schedules"] == (3 if compiled else 0)
+        plan.close()
+        runs.append(_focus(gpu_lib, sc, raw, compiled_schedules=compiled))
+    (out_a, slc_a, res_a), (out_b, slc_b, res_b) = runs
+    assert res_a["errors"] == res_b["errors"] == 0
+    assert np.array_equal(out_a, out_b)
+    assert np.array_equal(slc_a, slc_b)
