@@ -41,6 +41,7 @@ int backend_accc(const AcccArgs& a, int blocks, void* stream);
 int backend_rc_rows(const RcRowsArgs& a, int rows, LaunchShape sh, void* stream);
 int backend_multilook(const MultilookArgs& a, void* stream);
 int backend_ers_unpack(const ErsUnpackArgs& a, void* stream);
+int backend_asar_unpack(const AsarUnpackArgs& a, void* stream);
 int backend_rsl(const RslArgs& a, long long n, void* stream);
 int backend_srgr(const SrgrArgs& a, long long n, void* stream);
 

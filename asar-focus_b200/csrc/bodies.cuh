@@ -1247,6 +1247,42 @@ ASARF_HD ASARF_INLINE void ers_unpack_line(const ErsUnpackArgs& a, int y, int ti
     }
 }
 
+// Line y of an ASAR IM level-0 list: the sample blocks of its source packet (an echo packet;
+// a calibration line repeats the previous line's echo, as ParseEnvisatLevel0ImPackets copies
+// the previous record, envisat_format/src/envisat_im_parse.cc:599-615) become FBAQ4 record y:
+// the block-data length as a little-endian uint16 (the reference's memcpy of a uint16 on a
+// little-endian host), the blocks, zeros up to record_bytes.  SWST and PRI codes are the source
+// packet's.  The packet's data field header length (29) and mode ID (0x54) are checked as the
+// reference checks them (:470-484); a block length beyond the record sets kErrL0Length and the
+// record keeps only what fits.  Block y, threads over the record's bytes.
+ASARF_HD ASARF_INLINE void asar_unpack_line(const AsarUnpackArgs& a, int y, int tid, int nthr) {
+    const uint8_t* pk = a.mdsr + ASARF_LDG(a.src + y);
+    const int packet_length = (pk[36] << 8) | pk[37];
+    int len = packet_length - 29;
+    const int cap = a.record_bytes - 2;
+    unsigned e = 0;
+    if (((pk[38] << 8) | pk[39]) != 29) e |= kErrL0DataField;
+    if (pk[41] != 0x54) e |= kErrL0Mode;
+    if (len < 0 || len > cap) {
+        e |= kErrL0Length;
+        len = len < 0 ? 0 : cap;
+    }
+    uint8_t* rec = a.records + static_cast<long long>(y) * a.record_bytes;
+    const uint8_t* blocks = pk + kAsarPacketHeader;
+    for (int i = tid; i < a.record_bytes; i += nthr) {
+        uint8_t v;
+        if (i == 0) v = static_cast<uint8_t>(len & 0xFF);
+        else if (i == 1) v = static_cast<uint8_t>(len >> 8);
+        else v = (i - 2 < len) ? blocks[i - 2] : static_cast<uint8_t>(0);
+        rec[i] = v;
+    }
+    if (tid == 0) {
+        if (e) atomic_or_u32(a.errors, e);
+        if (a.pri) a.pri[y] = static_cast<uint16_t>((pk[54] << 8) | pk[55]);
+        if (a.swst) a.swst[y] = static_cast<uint16_t>((pk[56] << 8) | pk[57]);
+    }
+}
+
 // ----------------------------------------------------------------------------- L1 product records
 // Envisat MDS records of the level-1 products (ConditionResultsSLC / ConditionResultsDetected,
 // envisat_format/src/envisat_format_kernels.cu:28-114): `hdr` zero bytes of record header, then

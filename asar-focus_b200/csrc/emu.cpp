@@ -113,6 +113,11 @@ int backend_ers_unpack(const ErsUnpackArgs& a, void*) {
     return ASARF_OK;
 }
 
+int backend_asar_unpack(const AsarUnpackArgs& a, void*) {
+    for (int y = 0; y < a.lines; ++y) asar_unpack_line(a, y, 0, 1);
+    return ASARF_OK;
+}
+
 int backend_decode(const DecodeArgs& a, long long n, void*) {
     for (long long i = 0; i < n; ++i) decode_item(a, i);
     return ASARF_OK;

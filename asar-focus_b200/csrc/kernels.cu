@@ -355,6 +355,10 @@ __global__ void __launch_bounds__(256) k_ers_unpack(ErsUnpackArgs a) {
     ers_unpack_line(a, blockIdx.x, threadIdx.x, blockDim.x);
 }
 
+__global__ void __launch_bounds__(256) k_asar_unpack(AsarUnpackArgs a) {
+    asar_unpack_line(a, blockIdx.x, threadIdx.x, blockDim.x);
+}
+
 __global__ void __launch_bounds__(256) k_multilook(MultilookArgs a) {
     multilook_row_body(a, blockIdx.x, threadIdx.x, blockDim.x);
 }
@@ -581,6 +585,12 @@ int backend_ers_unpack(const ErsUnpackArgs& a, void* stream) {
     if (a.lines <= 0) return ASARF_OK;
     k_ers_unpack<<<a.lines, 256, 0, S(stream)>>>(a);
     return check_launch("ers_unpack");
+}
+
+int backend_asar_unpack(const AsarUnpackArgs& a, void* stream) {
+    if (a.lines <= 0) return ASARF_OK;
+    k_asar_unpack<<<a.lines, 256, 0, S(stream)>>>(a);
+    return check_launch("asar_unpack");
 }
 int backend_multilook(const MultilookArgs& a, void* stream) {
     k_multilook<<<a.out_y, 256, 0, S(stream)>>>(a);

@@ -302,6 +302,28 @@ struct ErsUnpackArgs {
     unsigned int* errors;     // kErrL0* bits
 };
 
+// ENVISAT ASAR IM source packets (ASA_IM__0P measurement data set, variable length):
+// 12 bytes ISP sensing time, 20 bytes FEP annotation (ISP length at 24), packet ID (32),
+// sequence control (34), packet length (36), data field header length 29 (38), then the data
+// field header (mode ID at 41, echo / noise / calibration flags at 52, PRI code at 54, SWST
+// code at 56) and the FBAQ4 sample blocks from byte 68 (packet length - 29 bytes).  The next
+// packet starts 39 + ISP length bytes after this one.
+constexpr int kAsarPacketHeader = 68;
+constexpr int kAsarNextPacketBase = 39;
+constexpr unsigned kErrL0DataField = 1u << 0;   // a packet's data field header length is not 29
+constexpr unsigned kErrL0Mode = 1u << 1;        // a packet's mode ID is not 0x54 (IM)
+constexpr unsigned kErrL0Length = 1u << 2;      // a packet's sample blocks do not fit the record
+struct AsarUnpackArgs {
+    const uint8_t* mdsr;      // packets, in file order
+    const long long* src;     // per line: byte offset of the echo packet whose sample blocks it holds
+    int lines;
+    int record_bytes;         // 2-byte length + the largest block-data length of the lines
+    uint8_t* records;         // [lines][record_bytes]: FBAQ4 records
+    uint16_t* swst;           // per line SWST code (nullable)
+    uint16_t* pri;            // per line PRI code (nullable)
+    unsigned int* errors;     // kErrL0DataField / kErrL0Mode / kErrL0Length bits
+};
+
 // ASAR FBAQ4 records -> complex rows, NaN where no sample (ConvertAsarImBlocksToComplex)
 struct DecodeFbaqArgs {
     const uint8_t* raw;

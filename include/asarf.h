@@ -297,6 +297,39 @@ int asarf_ers_l0_forecast(const uint8_t* mdsr, int64_t blob_bytes, int64_t num_d
 int asarf_ers_l0_unpack(const uint8_t* d_mdsr, const int64_t* d_offsets, int32_t lines, uint8_t* d_raw,
                         uint16_t* d_swst, uint16_t* d_pri, uint32_t* d_errors, void* stream);
 
+/* FetchEnvisatL0ImForecastMeta (envisat_format/src/envisat_im_parse.cc:297-385) over the
+ * measurement data set of an ASA_IM__0P product in host memory: `num_dsr` source packets of
+ * variable length from `mdsr` (each 39 + its FEP ISP length bytes; `blob_bytes` bounds the walk).
+ * Lines are the echo and calibration packets from the first echo packet on (noise packets
+ * skipped); the sensing-time window, counts and trimming as asarf_ers_l0_forecast, and a
+ * calibration packet left first after trimming is dropped (the reference accepts that only
+ * when the walk's last packet was a calibration packet, else ASARF_ERR_INVALID with its
+ * "Programming error" message).  A data field header length other than 29 is an error. */
+int asarf_asar_l0_forecast(const uint8_t* mdsr, int64_t blob_bytes, int64_t num_dsr, const asarf_mjd* start,
+                           const asarf_mjd* stop, int64_t* packets_before_start, int64_t* packets_after_stop,
+                           int64_t* offsets, asarf_mjd* times, int64_t capacity, int64_t* count);
+/* The host part of ParseEnvisatLevel0ImPackets (:387-676) for `count` forecast lines:
+ * *record_bytes = 2 + the largest echo block-data length (packet length - 29) over `count`
+ * consecutive packets from the first line's (ForecastMaxBlockDataLength, :159-197; fewer than
+ * 10 echo packets is an error); src_offsets[k] = the packet whose sample blocks line k holds
+ * (its own for an echo, the previous line's for a calibration packet), times[k] (nullable) its
+ * sensing time (a calibration line: the previous line's plus uint32(1 / (range_sampling_rate /
+ * PRI code) * 1e6) microseconds, in the reference's float arithmetic), *max_samples (nullable)
+ * the most samples a line holds.  Mode IDs other than 0x54 (IM) and the reference's other
+ * consistency failures are errors with its messages. */
+int asarf_asar_l0_lines(const uint8_t* mdsr, int64_t blob_bytes, const int64_t* offsets, int64_t count,
+                        float range_sampling_rate, int64_t* src_offsets, asarf_mjd* times, int32_t* record_bytes,
+                        int32_t* max_samples);
+/* The record copy of ParseEnvisatLevel0ImPackets on the GPU, one kernel for all `lines`: line y
+ * <- the sample blocks of the packet at d_mdsr + d_src_offsets[y] (device memory) as an FBAQ4
+ * record of `record_bytes` at d_records + y * record_bytes (2-byte little-endian block-data
+ * length, the blocks, zeros; the layout asarf_focus reads with raw_line_bytes = record_bytes),
+ * its SWST and PRI codes -> d_swst[y], d_pri[y] (nullable).  Bits of *d_errors (device memory,
+ * not cleared here): 0 data field header length not 29, 1 mode ID not 0x54, 2 block data longer
+ * than the record (the record keeps what fits).  Asynchronous on `stream`. */
+int asarf_asar_l0_unpack(const uint8_t* d_mdsr, const int64_t* d_src_offsets, int32_t lines, int32_t record_bytes,
+                         uint8_t* d_records, uint16_t* d_swst, uint16_t* d_pri, uint32_t* d_errors, void* stream);
+
 /* ---------------------------------------------------------------- host FP64 geometry */
 
 /* InterpolateOrbit (sar/orbit_state_vector.cc:23-48). */
