@@ -1008,11 +1008,11 @@ ASARF_HD ASARF_INLINE float bin_frequency(int f, int az_pad, float step) {
     return fmul_rn(static_cast<float>(k), step);
 }
 
-ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& cp, int x, int f, const float2* srow,
+// bf: the row's Doppler bin frequency (bin_frequency of its bin, from the block's row table).
+ASARF_HD ASARF_INLINE float2 rcmc_mf_sample(const AzRdArgs& a, const ColParams& cp, int x, float bf, const float2* srow,
                                             int cs, unsigned int* err_flag) {
     const float prf = a.prf;
     const float half = a.half_prf;
-    const float bf = bin_frequency(f, a.az_pad, a.bin_step);
     // --- aliased frequency (the same test decides the matched-filter band and the RCMC walk)
     float fn = bf;
     if (cp.dc < 0.0f) {
@@ -1093,32 +1093,33 @@ ASARF_HD ASARF_INLINE float2 az_abs_phase(const AzRdArgs& a, const ColParams& cp
 }
 
 // Shared-memory tables after the tile: column constants (xt), absolute-phase factors (xt),
-// row frequency bins (n2).
+// row bin frequencies (n2).
 ASARF_HD ASARF_INLINE float2* az_rd_phase_table(ColParams* cps, const AzRdArgs& a) {
     return reinterpret_cast<float2*>(cps + a.xt);
 }
-ASARF_HD ASARF_INLINE int* az_rd_bin_table(ColParams* cps, const AzRdArgs& a) {
-    return reinterpret_cast<int*>(az_rd_phase_table(cps, a) + a.xt);
+ASARF_HD ASARF_INLINE float* az_rd_freq_table(ColParams* cps, const AzRdArgs& a) {
+    return reinterpret_cast<float*>(az_rd_phase_table(cps, a) + a.xt);
 }
 
 // Per-block tables of the range-Doppler block, built while the tile is in flight: column
 // constants of the xt output columns (and their absolute-phase factors when asked for) and
-// the frequency bin of each of the n2 rows.
+// the Doppler bin frequency of each of the n2 rows (bin k1 + n1 drev2(p)).
 ASARF_HD ASARF_INLINE void az_rd_tables(const AzRdArgs& a, int tile, int k1, int tid, int nthr, ColParams* cps,
-                                        int* fbin) {
+                                        float* fbf) {
     const int x0 = tile * a.xt;
     float2* phs = az_rd_phase_table(cps, a);
     for (int c = tid; c < a.xt; c += nthr) {
         cps[c] = az_col_params(a, x0 + c);
         if (a.absolute_phase) phs[c] = az_abs_phase(a, cps[c], x0 + c);
     }
-    for (int p = tid; p < a.n2; p += nthr) fbin[p] = k1 + a.n1 * ASARF_LDG(a.drev2 + p);
+    for (int p = tid; p < a.n2; p += nthr)
+        fbf[p] = bin_frequency(k1 + a.n1 * ASARF_LDG(a.drev2 + p), a.az_pad, a.bin_step);
 }
 
-// Shared-memory bytes of the range-Doppler block: tile, column constants, phase factors, row bins.
+// Shared-memory bytes of the range-Doppler block: tile, column constants, phase factors, row frequencies.
 inline size_t az_rd_smem(int n2, int wt, int xt) {
     return sizeof(float2) * static_cast<size_t>(n2) * wt + sizeof(ColParams) * static_cast<size_t>(xt) +
-           sizeof(float2) * static_cast<size_t>(xt) + sizeof(int) * static_cast<size_t>(n2) + 16;
+           sizeof(float2) * static_cast<size_t>(xt) + sizeof(float) * static_cast<size_t>(n2) + 16;
 }
 
 // Right range halo of the range-Doppler block: the taps used (1 .. 14 of 16) reach 6 columns
@@ -1154,7 +1155,7 @@ struct AzRdOut {
 // transforms' radix schedule as compile-time constants (it must be the plan's).
 template <bool FWD = true, int R0 = 0, int R1 = 0, int R2 = 0>
 ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int tid, int nthr, float2* s,
-                                      const ColParams* cps, const int* fbin, unsigned int* err_flag, bool preloaded) {
+                                      const ColParams* cps, const float* fbf, unsigned int* err_flag, bool preloaded) {
     const int x0 = tile * a.xt;
     const int n2 = a.n2, wt = a.wt;
     const FastDiv dwt = make_fastdiv(static_cast<unsigned int>(wt));
@@ -1184,7 +1185,7 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
         // per sample, the 48-byte records cost 4-way bank conflicts on every field)
         const ColParams cp0 = cps[lane < a.xt ? lane : 0], cp1 = cps[lane + 32 < a.xt ? lane + 32 : 0];
         for (int p = warp; p < n2; p += nwarps) {
-            const int f = fbin[p];
+            const float f = fbf[p];
             const float2* srow = s + p * wt;
             float2 v0 = make_float2(0.0f, 0.0f), v1 = make_float2(0.0f, 0.0f);
             const int c0 = lane, c1 = lane + 32;
@@ -1206,7 +1207,7 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     {
         float2 rowbuf[64];
         for (int p = 0; p < n2; ++p) {
-            const int f = fbin[p];
+            const float f = fbf[p];
             for (int c = 0; c < a.xt; ++c) {
                 rowbuf[c] = (x0 + c < a.nk) ? rcmc_mf_sample(a, cps[c], x0 + c, f, s + p * wt, a.hl + c, err_flag)
                                             : make_float2(0.0f, 0.0f);

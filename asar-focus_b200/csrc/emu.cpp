@@ -93,11 +93,11 @@ int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, Launch
     TileBuf buf(sh.smem + 128);
     float2* s = buf.data();
     ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * a.wt);
-    int* fbin = az_rd_bin_table(cps, a);
+    float* fbf = az_rd_freq_table(cps, a);
     for (int b = 0; b < nblocks; ++b)
         for (int t = 0; t < tiles; ++t) {
-            az_rd_tables(a, t, b, 0, 1, cps, fbin);
-            az_rd_body(a, t, b, 0, 1, s, cps, fbin, err, false);
+            az_rd_tables(a, t, b, 0, 1, cps, fbf);
+            az_rd_body(a, t, b, 0, 1, s, cps, fbf, err, false);
         }
     return ASARF_OK;
 }

@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
     const int wt = a.wt;
     float2* s = reinterpret_cast<float2*>(smem_rd_raw);
     ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * wt);
-    int* fbin = az_rd_bin_table(cps, a);
+    float* fbf = az_rd_freq_table(cps, a);
     __shared__ uint64_t bar;
     if (a.use_tma && threadIdx.x == 0) {
         mbar_init(&bar, 1);
@@ -175,10 +175,10 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
             tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
     }
     // column constants and row bins are computed while the tile is in flight
-    az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbin);
+    az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbf);
     __syncthreads();
     if (a.use_tma) mbar_wait(&bar, 0, err);
-    az_rd_body<true, R0, R1, R2>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err,
+    az_rd_body<true, R0, R1, R2>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbf, err,
                                  a.use_tma != 0);
 }
 
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(512, 2) k_az_rd_split(AzRdArgs a, AzRdSplit sp
     float2* s = reinterpret_cast<float2*>(b_lo + kSplitMatrixBytes);
     const int wt = a.wt;
     ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * wt);
-    int* fbin = az_rd_bin_table(cps, a);
+    float* fbf = az_rd_freq_table(cps, a);
     __shared__ uint64_t bar, mbar;
     __shared__ uint32_t tmem_base;
     if (threadIdx.x < 32) tmem_alloc(&tmem_base, kSplitTmemCols);
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(512, 2) k_az_rd_split(AzRdArgs a, AzRdSplit sp
     const uint4* bsrc = reinterpret_cast<const uint4*>(sp.bmat);
     for (int i = threadIdx.x; i < 2 * kSplitMatrixBytes / 16; i += blockDim.x)
         reinterpret_cast<uint4*>(b_hi)[i] = __ldg(bsrc + i);
-    az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbin);
+    az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbf);
     fence_async_smem();  // B is read by the tensor cores
     tc_fence_before_sync();
     __syncthreads();
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(512, 2) k_az_rd_split(AzRdArgs a, AzRdSplit sp
     const uint32_t tmem = tmem_base;
     mbar_wait(&bar, 0, err);
     if (split_forward(a, sp, s, b_hi, b_lo, tmem, &mbar, err))
-        az_rd_body<false>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbin, err, true);
+        az_rd_body<false>(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, s, cps, fbf, err, true);
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
