@@ -907,13 +907,16 @@ ASARF_HD ASARF_INLINE void store_pair(float2* dst, int x, int nk, float2 u, floa
 template <int R0 = 0, int R1 = 0, int R2 = 0, int XT = 0>
 ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int b, int tid, int nthr, float2* s,
                                            const float2* tw, const int* rowmap, bool preloaded) {
-    const int x0 = tile * a.xt;
-    const int n1 = a.n1, xt = a.xt;
+    constexpr bool kCt = R0 > 0;
+    const int n1 = kCt ? R0 * R1 * R2 : a.n1, xt = kCt ? XT : a.xt;
+    const int x0 = tile * xt;
     const FastDiv dxt = make_fastdiv(static_cast<unsigned int>(xt));
+    // position t of the tile -> row (t / xt), by a constant when the schedule is compiled
+    auto row_of = [&](int t) { return kCt ? t / XT : static_cast<int>(fdiv_u(t, dxt)); };
     // tile [r][c] = row r*n2 + b, column x0 + c (natural order; columns >= nk read as 0)
     if (!preloaded) {
         for (int t = tid; t < n1 * xt; t += nthr) {
-            const int r = static_cast<int>(fdiv_u(t, dxt)), c = t - r * xt;
+            const int r = row_of(t), c = t - r * xt;
             const int row = r * a.n2 + b;
             const int x = x0 + c;
             float2 v = make_float2(0.0f, 0.0f);
@@ -934,7 +937,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
         else
             fft_forward_pairs<true, true>(a.plan1, s, xt, xt, tid, nthr);
         for (int t = tid; t < n1 * xt; t += nthr) {
-            const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
+            const int p = row_of(t), c = t - p * xt;
             const int x = x0 + c;
             if (x < a.nk) a.out[static_cast<long long>(rowmap[p]) * a.pitch + x] = cmul(s[t], tw[p]);
         }
@@ -947,7 +950,7 @@ ASARF_HD ASARF_INLINE void az_strided_body(const AzStridedArgs& a, int tile, int
         const int lo = a.state ? a.state->first_line : 0;
         const int hi = a.state ? lo + a.state->n_lines : n1 * a.n2;
         for (int t = tid; t < n1 * xt; t += nthr) {
-            const int p = static_cast<int>(fdiv_u(t, dxt)), c = t - p * xt;
+            const int p = row_of(t), c = t - p * xt;
             const int row = rowmap[p];
             const int x = x0 + c;
             if (x < a.nk && row >= lo && row < hi) {
