@@ -100,10 +100,12 @@ ASARF_HD inline bool polyfit_qr(const double* x, const double* y, int m, int deg
 // azimuth correlation per range block): the IQ correction is affine in the raw bytes,
 // so every sum the reference takes over corrected floats is a closed form of these.
 // Block (bx, by) covers kStatsCols work units and lines [by*L, (by+1)*L).  A unit is either
-// one column (general path) or, when the raw base and line stride are 8-byte aligned, a group
-// of 4 adjacent columns inside one Doppler block (quad path: one 8-byte window per line,
-// byte-lane dot products for all sums).  Either way every sum a thread keeps belongs to a
-// single Doppler block, and kStatsBatch lines are loaded before any is consumed.
+// one column (general path) or, when the raw base and line stride are 8-byte aligned, the
+// columns of one Doppler block inside an aligned group of 4 (quad path: columns 4g .. 4g + 3,
+// one aligned 8-byte load per line, byte-lane dot products for all sums; a group that straddles
+// a Doppler block boundary is two units, one per block, each masking the other's columns).
+// Either way every sum a thread keeps belongs to a single Doppler block, and kStatsBatch lines
+// are loaded before any is consumed.
 constexpr int kStatsCols = 256;
 constexpr int kStatsBatch = 8;
 constexpr int kStatsMaxLines = 256;
@@ -116,7 +118,7 @@ struct RawStatsSmem {
 
 // Host side: work units and grid width of the statistics kernel for this raw buffer.
 inline int raw_stats_grid_x(RawStatsArgs& a, const void* raw) {
-    a.gpb = (a.dc_step + 3) / 4;
+    a.gpb = (a.dc_step + 3) / 4 + 1;  // aligned groups a block's columns touch
     a.quad = (reinterpret_cast<uintptr_t>(raw) % 8 == 0 && a.line_bytes % 8 == 0) ? 1 : 0;
     const int units = a.quad ? a.nblk * a.gpb : a.nr;
     return (units + kStatsCols - 1) / kStatsCols;
@@ -250,31 +252,33 @@ ASARF_HD ASARF_INLINE void raw_stats_column(const RawStatsArgs& a, const RawStat
     lv[0] = l0, lv[1] = l1, lv[2] = l2, lv[3] = l3, lv[4] = l4, lv[5] = l5, lv[6] = l6, lv[7] = l7, lv[8] = l8;
 }
 
-// Quad path: columns x0 .. x0 + ncol - 1 (ncol <= 4, one Doppler block).  A line's four
-// samples are the 8 bytes (I0 Q0 I1 Q1 | I2 Q2 I3 Q3) at raw + y*line_bytes + 2*(x0 - off); their
-// offset inside an 8-byte word, o = 2*x0 mod 8, is the same on every line (the SWST shift is a
-// multiple of 4 samples), so two aligned 8-byte loads and a funnel shift fetch them.  Samples
-// outside the record or the group are masked to zero bytes, which drop out of every sum.
-ASARF_HD ASARF_INLINE void raw_stats_quad(const RawStatsArgs& a, const RawStatsSmem* sm, int x0, int ncol, int y0,
-                                          int y1, int ys, unsigned long long mv[6], unsigned int lv[9]) {
+// Quad path: the columns of `colmask` (bit k: column x0 + k) of the aligned group at x0
+// (x0 % 4 == 0), all in one Doppler block.  A line's four samples are the aligned 8 bytes
+// (I0 Q0 I1 Q1 | I2 Q2 I3 Q3) at raw + y*line_bytes + 2*(x0 - off) (the SWST shift is a
+// multiple of 4 samples, so the window stays aligned on every line).  Samples outside the
+// record or the mask are zero bytes, which drop out of every sum.
+ASARF_HD ASARF_INLINE void raw_stats_quad(const RawStatsArgs& a, const RawStatsSmem* sm, int x0, unsigned int colmask,
+                                          int y0, int y1, int ys, unsigned long long mv[6], unsigned int lv[9]) {
     constexpr unsigned int kLo = 0x00ff00ffu, kOnes = 0x01010101u;
-    const unsigned int colbits = (1u << ncol) - 1u;
-    const unsigned int o = static_cast<unsigned int>(2 * x0) & 7u;
-    const unsigned int sh = (o & 2u) * 8u;
-    const bool hi_word = (o & 4u) != 0;
+    const unsigned int colbits = colmask;
+    const int ncol = popc_u32(colmask);
     unsigned int cnt = 0, si = 0, sq = 0, sii = 0, sqq = 0, siq = 0;
     unsigned int l0 = 0, l1 = 0, l2 = 0, l3 = 0, l4 = 0, l5 = 0, l6 = 0, l7 = 0, l8 = 0;
     unsigned int pI0 = 0, pI1 = 0, pQ0 = 0, pQ1 = 0, pfb = 0;
-    const uint8_t* base = a.raw + 2ll * x0 - o;
+    const uint8_t* base = a.raw + 2ll * x0;
+    // byte masks of the group's columns: in the packed I (or Q) word byte k is column k; in the
+    // two raw words column k is the 16-bit lane k % 2 of word k / 2
+    const unsigned int cm = ((colmask & 1u) ? 0x000000ffu : 0u) | ((colmask & 2u) ? 0x0000ff00u : 0u) |
+                            ((colmask & 4u) ? 0x00ff0000u : 0u) | ((colmask & 8u) ? 0xff000000u : 0u);
     for (int yg = ys; yg < y1; yg += kStatsBatch) {
         // loads only in this loop (nothing consumes them), so all kStatsBatch lines are in flight
-        uint2 lo[kStatsBatch], hi[kStatsBatch];
+        uint2 w[kStatsBatch];
         unsigned int fbv[kStatsBatch];
         bool vec[kStatsBatch];
 #pragma unroll
         for (int u = 0; u < kStatsBatch; ++u) {
             const int y = yg + u;
-            lo[u] = hi[u] = make_uint2(0u, 0u);
+            w[u] = make_uint2(0u, 0u);
             fbv[u] = 0u;
             vec[u] = false;
             if (y < y1) {
@@ -282,20 +286,17 @@ ASARF_HD ASARF_INLINE void raw_stats_quad(const RawStatsArgs& a, const RawStatsS
                 const int i = x0 - off;
                 if (i >= 0 && i + 4 <= a.spl) {
                     // the whole 8-byte window is inside the record
-                    const uint2* p = reinterpret_cast<const uint2*>(base + static_cast<long long>(y) * a.line_bytes -
-                                                                    2ll * off);
-                    lo[u] = p[0];
-                    if (o != 0u) hi[u] = p[1];
+                    w[u] = *reinterpret_cast<const uint2*>(base + static_cast<long long>(y) * a.line_bytes - 2ll * off);
                     fbv[u] = colbits;
                     vec[u] = true;
                 } else {
-                    // record edge: sample by sample, words already assembled in lo
+                    // record edge: sample by sample
                     const uint8_t* row = a.raw + static_cast<long long>(y) * a.line_bytes;
-                    for (int k = 0; k < ncol; ++k) {
-                        if (i + k < 0 || i + k >= a.spl) continue;
+                    for (int k = 0; k < 4; ++k) {
+                        if (!((colbits >> k) & 1u) || i + k < 0 || i + k >= a.spl) continue;
                         const unsigned int v = *reinterpret_cast<const uint16_t*>(row + 2ll * (i + k));
-                        if (k < 2) lo[u].x |= v << (16 * k);
-                        else lo[u].y |= v << (16 * (k - 2));
+                        if (k < 2) w[u].x |= v << (16 * k);
+                        else w[u].y |= v << (16 * (k - 2));
                         fbv[u] |= 1u << k;
                     }
                 }
@@ -308,17 +309,12 @@ ASARF_HD ASARF_INLINE void raw_stats_quad(const RawStatsArgs& a, const RawStatsS
 #pragma unroll
         for (int u = 0; u < kStatsBatch; ++u) interior = interior && vec[u];
         if (interior) {
-            const unsigned int cm = ncol >= 4 ? 0xffffffffu : (1u << (8 * ncol)) - 1u;
             unsigned int pI = byte_perm(pI0, pI1, 0x6420u), pQ = byte_perm(pQ0, pQ1, 0x6420u);
             unsigned int psI = dp4(pI, kOnes, 0u), psQ = dp4(pQ, kOnes, 0u);
 #pragma unroll
             for (int u = 0; u < kStatsBatch; ++u) {
-                const unsigned int wa = hi_word ? lo[u].y : lo[u].x;
-                const unsigned int wb = hi_word ? hi[u].x : lo[u].y;
-                const unsigned int wc = hi_word ? hi[u].y : hi[u].x;
-                const unsigned int w0u = funnel_r(wa, wb, sh), w1u = funnel_r(wb, wc, sh);
-                const unsigned int I = byte_perm(w0u, w1u, 0x6420u) & cm;
-                const unsigned int Q = byte_perm(w0u, w1u, 0x7531u) & cm;
+                const unsigned int I = byte_perm(w[u].x, w[u].y, 0x6420u) & cm;
+                const unsigned int Q = byte_perm(w[u].x, w[u].y, 0x7531u) & cm;
                 const unsigned int sI = dp4(I, kOnes, 0u), sQ = dp4(Q, kOnes, 0u);
                 si += sI;
                 sq += sQ;
@@ -346,18 +342,10 @@ ASARF_HD ASARF_INLINE void raw_stats_quad(const RawStatsArgs& a, const RawStatsS
         for (int u = 0; u < kStatsBatch; ++u) {
             const int y = yg + u;
             if (y >= y1) break;
-            unsigned int w0u = lo[u].x, w1u = lo[u].y;
-            if (vec[u]) {
-                const unsigned int wa = hi_word ? lo[u].y : lo[u].x;
-                const unsigned int wb = hi_word ? hi[u].x : lo[u].y;
-                const unsigned int wc = hi_word ? hi[u].y : hi[u].x;
-                w0u = funnel_r(wa, wb, sh);
-                w1u = funnel_r(wb, wc, sh);
-            }
             const unsigned int fb = fbv[u];
             const unsigned int m0 = ((fb & 1u) ? 0x0000ffffu : 0u) | ((fb & 2u) ? 0xffff0000u : 0u);
             const unsigned int m1 = ((fb & 4u) ? 0x0000ffffu : 0u) | ((fb & 8u) ? 0xffff0000u : 0u);
-            const unsigned int c0 = w0u & m0, c1 = w1u & m1;
+            const unsigned int c0 = w[u].x & m0, c1 = w[u].y & m1;
             const unsigned int I0 = c0 & kLo, I1 = c1 & kLo;
             const unsigned int Q0 = (c0 >> 8) & kLo, Q1 = (c1 >> 8) & kLo;
             if (y >= y0) {
@@ -417,12 +405,17 @@ ASARF_HD ASARF_INLINE void raw_stats_body(const RawStatsArgs& a, int bx, int by,
         bool valid;
         int blk;
         if (a.quad) {
+            // group k of Doppler block blk: the aligned group at (block start & ~3) + 4k, the
+            // block's columns [xs, xe) in it
             blk = static_cast<int>(fdiv_u(static_cast<unsigned int>(unit), dgpb));
-            const int x0 = blk * a.dc_step + 4 * (unit - blk * a.gpb);
+            const int xs = blk * a.dc_step;
             const int xe = (blk + 1) * a.dc_step < a.nr ? (blk + 1) * a.dc_step : a.nr;
-            const int ncol = xe - x0 < 4 ? xe - x0 : 4;
-            valid = blk < a.nblk && ncol > 0;
-            if (valid) raw_stats_quad(a, sm, x0, ncol, y0, y1, ys, mv, lv);
+            const int x0 = (xs & ~3) + 4 * (unit - blk * a.gpb);
+            const int c_lo = xs > x0 ? xs - x0 : 0;
+            const int c_hi = xe - x0 < 4 ? xe - x0 : 4;
+            valid = blk < a.nblk && c_hi > c_lo;
+            const unsigned int colmask = valid ? ((1u << c_hi) - 1u) & ~((1u << c_lo) - 1u) : 0u;
+            if (valid) raw_stats_quad(a, sm, x0, colmask, y0, y1, ys, mv, lv);
         } else {
             valid = unit < a.nr;
             blk = valid ? static_cast<int>(fdiv_u(static_cast<unsigned int>(unit), dstep)) : 0;
