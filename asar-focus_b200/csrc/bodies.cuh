@@ -1387,39 +1387,70 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
         const float2 w = base[o];
         return fma_rn(w.x, w.x, fmul_rn(w.y, w.y));
     };
-    for (int cb = tid; cb < a.nx; cb += 2 * nthr) {
-        float v[2][kTailRows];
+    // column c from its window rows v[0 .. kTailRows) (rows r_lo + k; later rows, when the window
+    // is longer, read here): both box means, their interpolation and the range spreading loss
+    auto finish = [&](int c, const float* v) {
+        float sum0 = 0.0f, sum1 = 0.0f;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int c = cb + h * nthr;
-#pragma unroll
-            for (int k = 0; k < kTailRows; ++k) {
-                v[h][k] = 0.0f;
-                if (k < nr && c < a.nx) v[h][k] = power(r_lo + k, c);
-            }
+        for (int k = 0; k < kTailRows; ++k) {
+            const int r = r_lo + k;
+            if (k >= nr) break;
+            if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, v[k]);
+            if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, v[k]);
         }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int c = cb + h * nthr;
-            if (c >= a.nx) break;
-            float sum0 = 0.0f, sum1 = 0.0f;
+        for (int r = r_lo + kTailRows; r < r_hi; ++r) {
+            const float p2 = power(r, c);
+            if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
+            if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
+        }
+        if (c0) sum0 = div_by_recip_rn(sum0, fc0, rc0);
+        if (c1) sum1 = div_by_recip_rn(sum1, fc1, rc1);
+        float val = 0.0f;
+        if (c0 && c1) val = fma_rn(fsub_rn(sum1, sum0), mu, sum0);
+        ml[c] = fmul_rn(val, ASARF_LDG(tv.rsl + c));
+    };
+    // |z|^2 rows with 16-byte aligned rows: four adjacent columns per thread, one 16-byte load per row
+    const bool quad = ibase && (a.nx & 3) == 0 && (a.pitch & 3) == 0 && (reinterpret_cast<uintptr_t>(ibase) & 15) == 0;
+    if (quad) {
+        for (int q = tid; q < a.nx / 4; q += nthr) {
+            float4 w[kTailRows];
 #pragma unroll
             for (int k = 0; k < kTailRows; ++k) {
-                const int r = r_lo + k;
-                if (k >= nr) break;
-                if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, v[h][k]);
-                if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, v[h][k]);
+                w[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (k < nr) w[k] = *reinterpret_cast<const float4*>(ibase + static_cast<long long>(r_lo + k) * a.pitch + 4 * q);
             }
-            for (int r = r_lo + kTailRows; r < r_hi; ++r) {
-                const float p2 = power(r, c);
-                if (r >= s0 && r < e0) sum0 = fadd_rn(sum0, p2);
-                if (r >= s1 && r < e1) sum1 = fadd_rn(sum1, p2);
+            float v[kTailRows];
+#pragma unroll
+            for (int k = 0; k < kTailRows; ++k) v[k] = w[k].x;
+            finish(4 * q, v);
+#pragma unroll
+            for (int k = 0; k < kTailRows; ++k) v[k] = w[k].y;
+            finish(4 * q + 1, v);
+#pragma unroll
+            for (int k = 0; k < kTailRows; ++k) v[k] = w[k].z;
+            finish(4 * q + 2, v);
+#pragma unroll
+            for (int k = 0; k < kTailRows; ++k) v[k] = w[k].w;
+            finish(4 * q + 3, v);
+        }
+    } else {
+        for (int cb = tid; cb < a.nx; cb += 2 * nthr) {
+            float v[2][kTailRows];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = cb + h * nthr;
+#pragma unroll
+                for (int k = 0; k < kTailRows; ++k) {
+                    v[h][k] = 0.0f;
+                    if (k < nr && c < a.nx) v[h][k] = power(r_lo + k, c);
+                }
             }
-            if (c0) sum0 = div_by_recip_rn(sum0, fc0, rc0);
-            if (c1) sum1 = div_by_recip_rn(sum1, fc1, rc1);
-            float val = 0.0f;
-            if (c0 && c1) val = fma_rn(fsub_rn(sum1, sum0), mu, sum0);
-            ml[c] = fmul_rn(val, ASARF_LDG(tv.rsl + c));
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = cb + h * nthr;
+                if (c >= a.nx) break;
+                finish(c, v[h]);
+            }
         }
     }
     ASARF_SYNC();
