@@ -165,9 +165,10 @@ def _describe(sc) -> str:
     return f"{kind} {sc.range_size} range x {sc.azimuth_size} azimuth, {fmt}, {grid}, {dc}, {vr}"
 
 
-def make_scene(workload: str, seed: int):
+def make_scene(workload: str, seed: int, azimuth_size: int = 0):
+    """The workload's scene; azimuth_size > 0 cuts it to that many lines (profiling cases)."""
     from asarf import scene as S
-    return S.WORKLOADS[workload](seed=seed)
+    return S.WORKLOADS[workload](seed=seed, **({"azimuth_size": azimuth_size} if azimuth_size else {}))
 
 
 def algorithmic_bytes(sc, dims: dict, res: dict) -> dict:
@@ -422,7 +423,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     from asarf import sim
 
     lib = asarf.load_library()
-    sc = make_scene(args.workload, 1001 + rank)
+    sc = make_scene(args.workload, 1001 + rank, args.azimuth_size)
     sc.prepare(lib)
     prec = 1 if args.precision == "split" else 0
     raw_np, _ = sim.simulate(sc, device="cuda")
@@ -442,6 +443,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                          "candidates": [[o, None if m is None else round(m, 4)] for o, m in entry["timings"]]}
     # the product is the detected image: no complex SLC is kept (|z|^2 rows feed the multilook)
     tuned = dict(tuned, keep_slc=False)
+    if args.az_n2:
+        tuned["az_n2"] = args.az_n2
     plan = asarf.FocusPlan(sc, lib=lib, **dict(tuned, precision=prec))
     out_d = torch.empty(plan.out_shape, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
@@ -852,6 +855,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other precision form")
     ap.add_argument("--no-tune", action="store_true", help="the planner's launch shapes, no timed autotuning")
     ap.add_argument("--no-workloads", action="store_true", help="skip timing the other configurations")
+    ap.add_argument("--azimuth-size", type=int, default=0,
+                    help="cut the workload's scene to this many lines (profiling cases; 0 = as defined)")
+    ap.add_argument("--az-n2", type=int, default=0,
+                    help="contiguous azimuth transform length of the plan (profiling cases; 0 = planner/tuner)")
     ap.add_argument("--precision", choices=["fp32", "split"], default="fp32",
                     help="azimuth transform form: plain FP32, or tensor-core bf16 hi+lo DFT tiles")
     args = ap.parse_args()
