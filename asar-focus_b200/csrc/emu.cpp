@@ -78,18 +78,30 @@ int backend_range_compress(const RangeCompressArgs& a, int lines, LaunchShape sh
     return ASARF_OK;
 }
 
-int backend_az_strided(const AzStridedArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, void*) {
+// The same instantiation choice as the device backend (strided_schedule_compiled).
+template <int R0, int R1, int R2, int XT>
+static void emu_az_strided(const AzStridedArgs& a, int tiles, int nblocks, LaunchShape sh) {
     TileBuf s(sh.smem);
     float2* tw = s.data() + static_cast<size_t>(a.n1) * a.xt;
     int* row = reinterpret_cast<int*>(tw + a.n1);
     for (int b = 0; b < nblocks; ++b) {
         az_strided_tables(a, b, 0, 1, tw, row);
-        for (int t = 0; t < tiles; ++t) az_strided_body(a, t, b, 0, 1, s.data(), tw, row, false);
+        for (int t = 0; t < tiles; ++t) az_strided_body<R0, R1, R2, XT>(a, t, b, 0, 1, s.data(), tw, row, false);
+    }
+}
+
+int backend_az_strided(const AzStridedArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, void*) {
+    if (a.compiled && strided_schedule_compiled(a.plan1, a.xt)) {
+        if (plan_is(a.plan1, 9, 5, 5)) emu_az_strided<9, 5, 5, 32>(a, tiles, nblocks, sh);
+        else emu_az_strided<9, 4, 5, 32>(a, tiles, nblocks, sh);
+    } else {
+        emu_az_strided<0, 0, 0, 0>(a, tiles, nblocks, sh);
     }
     return ASARF_OK;
 }
 
-int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void*) {
+template <int R0, int R1, int R2>
+static void emu_az_rd(const AzRdArgs& a, int tiles, int nblocks, LaunchShape sh, unsigned int* err) {
     TileBuf buf(sh.smem + 128);
     float2* s = buf.data();
     ColParams* cps = reinterpret_cast<ColParams*>(s + static_cast<size_t>(a.n2) * a.wt);
@@ -97,8 +109,18 @@ int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, Launch
     for (int b = 0; b < nblocks; ++b)
         for (int t = 0; t < tiles; ++t) {
             az_rd_tables(a, t, b, 0, 1, cps, fbf);
-            az_rd_body(a, t, b, 0, 1, s, cps, fbf, err, false);
+            az_rd_body<true, R0, R1, R2>(a, t, b, 0, 1, s, cps, fbf, err, false);
         }
+}
+
+// The same instantiation choice as the device backend (block_schedule_compiled).
+int backend_az_rd(const AzRdArgs& a, const void*, int tiles, int nblocks, LaunchShape sh, unsigned int* err, void*) {
+    if (a.compiled && block_schedule_compiled(a.plan2)) {
+        if (plan_is(a.plan2, 5, 5, 5)) emu_az_rd<5, 5, 5>(a, tiles, nblocks, sh, err);
+        else emu_az_rd<8, 7, 3>(a, tiles, nblocks, sh, err);
+    } else {
+        emu_az_rd<0, 0, 0>(a, tiles, nblocks, sh, err);
+    }
     return ASARF_OK;
 }
 

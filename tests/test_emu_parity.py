@@ -106,3 +106,24 @@ def test_detected_only_runs_equal_the_kept_slc_runs(emu_lib):
     assert np.array_equal(det, full)
     with pytest.raises(_lib.AsarfError):
         plan.slc_into(np.zeros((4, 4), dtype=np.complex64))
+
+
+# (azimuth lines, az_n2, compiled_schedules bits): scenes whose transforms take each compiled
+# instantiation -- blocks 125 = 5*5*5 and 168 = 8*7*3, strided 225 = 9*5*5 and 180 = 9*4*5
+COMPILED_CASES = [(1990, 125, 2), (3590, 16, 1), (2010, 168, 2), (2870, 16, 1)]
+
+
+@pytest.mark.parametrize("lines, n2, bits", COMPILED_CASES)
+def test_compiled_schedules_equal_run_time_schedules(emu_lib, lines, n2, bits):
+    """The compile-time transform schedules run the same operations in the same order as the
+    run-time ones: identical images, and the compiled run matches the oracle."""
+    sc, raw, _ = scene_and_raw(emu_lib, S.tiny, azimuth_size=lines, seed=3)
+    outs = []
+    for compiled in (True, False):
+        plan = asarf.FocusPlan(sc, lib=emu_lib, az_n2=n2, compiled_schedules=compiled)
+        assert plan.dims["compiled_schedules"] == (bits if compiled else 0)
+        outs.append(plan.focus_host(raw))
+        assert plan.results()["errors"] == 0
+    assert np.array_equal(outs[0], outs[1])
+    if lines == 1990:
+        assert rel_rmse(outs[0], oracle_focus(sc, raw).detected) < TOL_DETECTED

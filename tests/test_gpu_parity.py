@@ -165,3 +165,17 @@ def test_detected_only_runs_equal_the_kept_slc_runs(gpu_lib, factory):
     full = asarf.FocusPlan(sc, lib=gpu_lib).focus_host(raw)
     det = asarf.FocusPlan(sc, lib=gpu_lib, keep_slc=False).focus_host(raw)
     assert np.array_equal(det, full)
+
+
+@pytest.mark.parametrize("lines, n2, bits", [(1990, 125, 2), (3590, 16, 1), (2010, 168, 2), (2870, 16, 1)])
+def test_compiled_schedules_equal_run_time_schedules(gpu_lib, lines, n2, bits):
+    """Every compiled instantiation (blocks 125 / 168, strided 225 / 180) on the GPU: the same
+    image as the run-time schedules, bit for bit."""
+    sc, raw, _ = scene_and_raw(gpu_lib, S.tiny, azimuth_size=lines, seed=3)
+    outs = []
+    for compiled in (True, False):
+        plan, out, res = _focus(gpu_lib, sc, raw, az_n2=n2, compiled_schedules=compiled)
+        assert plan.dims["compiled_schedules"] == (bits if compiled else 0)
+        assert res["errors"] == 0
+        outs.append(out)
+    assert np.array_equal(outs[0], outs[1])
