@@ -265,7 +265,7 @@ extern "C" int asarf_raw_statistics_noalloc(const uint8_t* d_raw, int32_t raw_li
     st.min_swst = min_swst;
     st.dc_step = dc_step;
     st.nblk = nblk;
-    st.lines_per_cta = kStatsMaxLines / 4;
+    st.lines_per_cta = kStatsLinesPerBlock;
     st.acc = &g_emu_scratch.acc;
     backend_raw_stats(st, raw_stats_grid_x(st, d_raw), (azimuth_size + st.lines_per_cta - 1) / st.lines_per_cta,
                       nullptr);

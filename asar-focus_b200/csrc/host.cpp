@@ -842,7 +842,7 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     st.nr = p->nr;
     st.dc_step = dc_step;
     st.nblk = nblk;
-    st.lines_per_cta = kStatsMaxLines / 4;
+    st.lines_per_cta = kStatsLinesPerBlock;
     st.acc = p->acc;
     p->stats_gy = (p->na + st.lines_per_cta - 1) / st.lines_per_cta;
     if (fbaq) {
