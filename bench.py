@@ -442,7 +442,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                          "ms_tuned": round(entry["ms_tuned"], 4), "seconds": round(time.perf_counter() - t_tune, 1),
                          "candidates": [[o, None if m is None else round(m, 4)] for o, m in entry["timings"]]}
     # the product is the detected image: no complex SLC is kept (|z|^2 rows feed the multilook)
-    tuned = dict(tuned, keep_slc=False)
+    tuned = dict(tuned, keep_slc=bool(args.keep_slc))
     if args.az_n2:
         tuned["az_n2"] = args.az_n2
     plan = asarf.FocusPlan(sc, lib=lib, **dict(tuned, precision=prec))
@@ -554,6 +554,9 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
                    "launch_shapes": {"az_n2": dims["n2"], "az_tile_width": dims["az_tile_width"],
                                      "strided_tile_width": dims["strided_tile_width"],
                                      "rc_fft_len": dims["rc_fft_len"]},
+                   "compiled_schedules": dims["compiled_schedules"],
+                   "product": "detected image" + (" (complex SLC kept)" if args.keep_slc else
+                                                  " (no complex SLC kept: |z|^2 rows feed the multilook)"),
                    "autotune": tune_info},
         "e2e": e2e,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -857,6 +860,8 @@ def main():
     ap.add_argument("--no-workloads", action="store_true", help="skip timing the other configurations")
     ap.add_argument("--azimuth-size", type=int, default=0,
                     help="cut the workload's scene to this many lines (profiling cases; 0 = as defined)")
+    ap.add_argument("--keep-slc", action="store_true",
+                    help="keep the complex SLC in device memory (the library's default; the headline run does not)")
     ap.add_argument("--az-n2", type=int, default=0,
                     help="contiguous azimuth transform length of the plan (profiling cases; 0 = planner/tuner)")
     ap.add_argument("--precision", choices=["fp32", "split"], default="fp32",
