@@ -328,10 +328,15 @@ extern "C" int asarf_asar_l0_lines(const uint8_t* mdsr, int64_t blob_bytes, cons
             return set_error(ASARF_ERR_INVALID, "Expected only IM mode packets, but encountered mode ID %#x",
                              static_cast<unsigned>(h.mode));
         if (h.echo()) {
+            // the unpack kernel reads the packet's blocks from the device copy of this data set
+            const int64_t blocks = static_cast<uint16_t>(h.packet_length - 29);
+            if (offsets[k] + kAsarPacketHeader + blocks > blob_bytes)
+                return set_error(ASARF_ERR_INVALID, "asar_l0_lines: line %lld's sample blocks end past the data set",
+                                 static_cast<long long>(k));
             src_offsets[k] = offsets[k];
             if (times) times[k] = h.time;
             last_pri = h.pri;
-            const int64_t n = fbaq_block_samples(static_cast<uint16_t>(h.packet_length - 29));
+            const int64_t n = fbaq_block_samples(blocks);
             if (n > most) most = n;
         } else if (h.cal()) {
             // the previous line repeated, its sensing time advanced by one PRI in whole

@@ -316,7 +316,8 @@ int asarf_asar_l0_forecast(const uint8_t* mdsr, int64_t blob_bytes, int64_t num_
  * sensing time (a calibration line: the previous line's plus uint32(1 / (range_sampling_rate /
  * PRI code) * 1e6) microseconds, in the reference's float arithmetic), *max_samples (nullable)
  * the most samples a line holds.  Mode IDs other than 0x54 (IM) and the reference's other
- * consistency failures are errors with its messages. */
+ * consistency failures are errors with its messages, and so is an echo packet whose sample
+ * blocks end past blob_bytes (the unpack kernel reads them from the device copy). */
 int asarf_asar_l0_lines(const uint8_t* mdsr, int64_t blob_bytes, const int64_t* offsets, int64_t count,
                         float range_sampling_rate, int64_t* src_offsets, asarf_mjd* times, int32_t* record_bytes,
                         int32_t* max_samples);

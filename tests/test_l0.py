@@ -220,6 +220,11 @@ def test_asar_rejects_the_reference_error_cases(emu_lib):
     assert b"Programming error detected" in emu_lib.asarf_last_error()
     with pytest.raises(ValueError):
         ol0.asar_forecast(blob, num, l0.mjd(T0_US + 20 * 605), (10**6, 0, 0), 0, 0)
+    # a data set cut inside the last echo packet's sample blocks
+    offs, _, _, _ = l0.asar_forecast(blob, num, (0, 0, 0), (10**6, 0, 0), 0, 0, lib=emu_lib)
+    with pytest.raises(_lib.AsarfError):
+        l0.asar_lines(blob[:-10], offs, RSR, lib=emu_lib)
+    assert b"end past the data set" in emu_lib.asarf_last_error()
     # the unpack kernel flags a block length beyond the record
     offs, _, _, _ = l0.asar_forecast(blob, num, (0, 0, 0), (10**6, 0, 0), 0, 0, lib=emu_lib)
     src, _, record_bytes, _ = l0.asar_lines(blob, offs, RSR, lib=emu_lib)
