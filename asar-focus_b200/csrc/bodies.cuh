@@ -1415,15 +1415,34 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
         if (c0 && c1) val = fma_rn(fsub_rn(sum1, sum0), mu, sum0);
         ml[c] = fmul_rn(val, ASARF_LDG(tv.rsl + c));
     };
-    // |z|^2 rows with 16-byte aligned rows: four adjacent columns per thread, one 16-byte load per row
-    const bool quad = ibase && (a.nx & 3) == 0 && (a.pitch & 3) == 0 && (reinterpret_cast<uintptr_t>(ibase) & 15) == 0;
+    // 16-byte aligned rows: four adjacent columns per thread, one 16-byte load per row of |z|^2
+    // floats, or two of complex samples (|z|^2 formed with the same rounding as power())
+    const bool quad = (a.nx & 3) == 0 && (a.pitch & 3) == 0 &&
+                      (ibase ? (reinterpret_cast<uintptr_t>(ibase) & 15) == 0
+                             : (reinterpret_cast<uintptr_t>(base) & 15) == 0);
     if (quad) {
         for (int q = tid; q < a.nx / 4; q += nthr) {
             float4 w[kTailRows];
+            if (ibase) {
 #pragma unroll
-            for (int k = 0; k < kTailRows; ++k) {
-                w[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if (k < nr) w[k] = *reinterpret_cast<const float4*>(ibase + static_cast<long long>(r_lo + k) * a.pitch + 4 * q);
+                for (int k = 0; k < kTailRows; ++k) {
+                    w[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    if (k < nr)
+                        w[k] = *reinterpret_cast<const float4*>(ibase + static_cast<long long>(r_lo + k) * a.pitch + 4 * q);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < kTailRows; ++k) {
+                    float4 z0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), z1 = z0;
+                    if (k < nr) {
+                        const float4* p =
+                            reinterpret_cast<const float4*>(base + static_cast<long long>(r_lo + k) * a.pitch + 4 * q);
+                        z0 = p[0];
+                        z1 = p[1];
+                    }
+                    w[k] = make_float4(fma_rn(z0.x, z0.x, fmul_rn(z0.y, z0.y)), fma_rn(z0.z, z0.z, fmul_rn(z0.w, z0.w)),
+                                       fma_rn(z1.x, z1.x, fmul_rn(z1.y, z1.y)), fma_rn(z1.z, z1.z, fmul_rn(z1.w, z1.w)));
+                }
             }
             float v[kTailRows];
 #pragma unroll
