@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(512) k_az_rd(AzRdArgs a, unsigned int* err, co
         for (int r0 = 0; r0 < a.n2; r0 += a.n2_box)
             tma_load_2d(s + static_cast<size_t>(r0) * wt, &map, &bar, x, blockIdx.y * a.n2 + r0);
     }
-    // column constants and row bins are computed while the tile is in flight
+    // column constants and row frequencies are computed while the tile is in flight
     az_rd_tables(a, blockIdx.x, blockIdx.y, threadIdx.x, blockDim.x, cps, fbf);
     __syncthreads();
     if (a.use_tma) mbar_wait(&bar, 0, err);
