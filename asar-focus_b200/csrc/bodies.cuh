@@ -1152,6 +1152,16 @@ struct AzRdOut {
     }
 };
 
+// Packed twiddle products in the range-Doppler block's n2 transforms: for schedules of radices
+// <= 5 only (ERS 5 x 5 x 5: 1.483 -> 1.460 ms; ASAR IM 8 x 7 x 3 measured slower with them,
+// 1.604 -> 1.683 ms).  The compiled and run-time schedules apply the same rule, so they give
+// identical results.
+ASARF_HD ASARF_INLINE bool az_rd_packed_twiddles(const FftPlan& p) {
+    bool small = true;
+    for (int i = 0; i < p.nst; ++i) small = small && p.radix[i] <= 5;
+    return small;
+}
+
 // FWD = false: the caller has already put the tile through the forward transform (the
 // split-precision kernel's tensor-core DFT) and synchronised.  R0, R1, R2 > 0: the n2
 // transforms' radix schedule as compile-time constants (it must be the plan's).
@@ -1173,9 +1183,11 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
     if constexpr (FWD) {
         ASARF_SYNC();
         if constexpr (R0 > 0)
-            fft_forward_pairs_cs3<R0, R1, R2>(s, wt, wt, a.plan2.tw, tid, nthr);
+            fft_forward_pairs_cs3<R0, R1, R2, (R0 <= 5 && R1 <= 5 && R2 <= 5)>(s, wt, wt, a.plan2.tw, tid, nthr);
+        else if (az_rd_packed_twiddles(a.plan2))
+            fft_forward_pairs<false, true>(a.plan2, s, wt, wt, tid, nthr);
         else
-            fft_forward_pairs(a.plan2, s, wt, wt, tid, nthr);
+            fft_forward_pairs<false, false>(a.plan2, s, wt, wt, tid, nthr);
     }
     // RCMC + matched filter.  Every output (row p, column c) reads taps of row p only, so a
     // row is computed into registers by one warp (lane = column, xt <= 64), the warp
@@ -1221,9 +1233,12 @@ ASARF_HD ASARF_INLINE void az_rd_body(const AzRdArgs& a, int tile, int k1, int t
 #endif
     // the inverse transform's last stage stores the block's rows k1 * n2 + r directly
     if constexpr (R0 > 0)
-        fft_inverse_pairs_cs3<R0, R1, R2>(s + a.hl, a.xt, wt, a.plan2.tw, tid, nthr, AzRdOut{&a, x0, k1});
+        fft_inverse_pairs_cs3<R0, R1, R2, AzRdOut, (R0 <= 5 && R1 <= 5 && R2 <= 5)>(s + a.hl, a.xt, wt, a.plan2.tw,
+                                                                                   tid, nthr, AzRdOut{&a, x0, k1});
+    else if (az_rd_packed_twiddles(a.plan2))
+        fft_inverse_pairs<AzRdOut, true>(a.plan2, s + a.hl, a.xt, wt, tid, nthr, AzRdOut{&a, x0, k1});
     else
-        fft_inverse_pairs(a.plan2, s + a.hl, a.xt, wt, tid, nthr, AzRdOut{&a, x0, k1});
+        fft_inverse_pairs<AzRdOut, false>(a.plan2, s + a.hl, a.xt, wt, tid, nthr, AzRdOut{&a, x0, k1});
 }
 
 // ----------------------------------------------------------------------------- ERS level-0 packets
@@ -1417,9 +1432,9 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
     };
     // 16-byte aligned rows: four adjacent columns per thread, one 16-byte load per row of |z|^2
     // floats, or two of complex samples (|z|^2 formed with the same rounding as power())
-    const bool quad = (a.nx & 3) == 0 && (a.pitch & 3) == 0 &&
-                      (ibase ? (reinterpret_cast<uintptr_t>(ibase) & 15) == 0
-                             : (reinterpret_cast<uintptr_t>(base) & 15) == 0);
+    // (columns past the last whole group of four, when nx is not a multiple of 4, one per thread)
+    const bool quad = (a.pitch & 3) == 0 && (ibase ? (reinterpret_cast<uintptr_t>(ibase) & 15) == 0
+                                                   : (reinterpret_cast<uintptr_t>(base) & 15) == 0);
     if (quad) {
         for (int q = tid; q < a.nx / 4; q += nthr) {
             float4 w[kTailRows];
@@ -1457,6 +1472,12 @@ ASARF_HD ASARF_INLINE void tail_body(const TailArgs& a, int y, int tid, int nthr
 #pragma unroll
             for (int k = 0; k < kTailRows; ++k) v[k] = w[k].w;
             finish(4 * q + 3, v);
+        }
+        for (int c = (a.nx & ~3) + tid; c < a.nx; c += nthr) {
+            float v[kTailRows];
+#pragma unroll
+            for (int k = 0; k < kTailRows; ++k) v[k] = k < nr ? power(r_lo + k, c) : 0.0f;
+            finish(c, v);
         }
     } else {
         for (int cb = tid; cb < a.nx; cb += 2 * nthr) {

@@ -517,8 +517,8 @@ ASARF_HD ASARF_INLINE void fft_stage_pair_ct(float2* s, const float2* __restrict
 
 // The same stage with the length N and span S compile-time constants and the column count
 // run-time (npair pairs, divider pdiv, row stride ldc): the range-Doppler block, whose tile
-// width follows the scene's range walk.
-template <int R, bool INV, bool TW_FIRST, int N, int S, class Epi = NoEpi>
+// width follows the scene's range walk.  PTW: packed twiddle products.
+template <int R, bool INV, bool TW_FIRST, int N, int S, class Epi = NoEpi, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair_cs(float2* s, int npair, const FastDiv& pdiv, int ldc,
                                              const float2* __restrict__ tw, int tid, int nthr,
                                              const Epi& epi = Epi()) {
@@ -529,7 +529,7 @@ ASARF_HD ASARF_INLINE void fft_stage_pair_cs(float2* s, int npair, const FastDiv
         const int cp = t - bj * npair;
         const int b = bj / S;
         const int j = bj - b * S;
-        pair_item<R, INV, TW_FIRST, false, Epi, false>(s, b, j, cp, M, S, ldc, N / M, tw, nullptr, epi);
+        pair_item<R, INV, TW_FIRST, false, Epi, PTW>(s, b, j, cp, M, S, ldc, N / M, tw, nullptr, epi);
     }
 }
 
@@ -539,8 +539,8 @@ ASARF_HD ASARF_INLINE void fft_stage_pair_cs(float2* s, int npair, const FastDiv
 // NINE adds radix 9 (two radix-3 DFTs in registers, 36 values per column pair: 71 registers
 // in the strided kernel, whose occupancy shared memory limits anyway) for plans that merge
 // factors 3 * 3; it is compiled only where such plans run, since every extra case costs the
-// other kernels registers.  PTW selects the packed twiddle products (measured faster in the
-// strided kernel, slower in the range-Doppler block at its 64-register bound).
+// other kernels registers.  PTW selects the packed twiddle products: the strided kernel uses them,
+// the range-Doppler block for radix <= 5 schedules only (az_rd_packed_twiddles).
 template <bool INV, bool TW_FIRST, bool NINE = false, bool PRE = false, class Epi = NoEpi, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_stage_pair_dispatch(int R, float2* s, int n, int S, const FastDiv& sdiv, int npair,
                                                    const FastDiv& pdiv, int ldc, const float2* __restrict__ tw,
@@ -578,18 +578,18 @@ ASARF_HD ASARF_INLINE void fft_forward_pairs(const FftPlan& p, float2* s, int nc
 }
 
 // With an active epilogue the last stage writes through it and the tile is left unfinished.
-template <class Epi = NoEpi>
+template <class Epi = NoEpi, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_inverse_pairs(const FftPlan& p, float2* s, int ncol, int ldc, int tid, int nthr,
                                              const Epi& epi = Epi()) {
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
     for (int i = p.nst - 1; i >= 0; --i) {
         if (Epi::kActive && i == 0)
-            fft_stage_pair_dispatch<true, true, false, false, Epi>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair,
-                                                                   pdiv, ldc, p.tw, tid, nthr, nullptr, epi);
+            fft_stage_pair_dispatch<true, true, false, false, Epi, PTW>(p.radix[i], s, p.n, p.span[i], p.sdiv[i],
+                                                                        npair, pdiv, ldc, p.tw, tid, nthr, nullptr, epi);
         else
-            fft_stage_pair_dispatch<true, true>(p.radix[i], s, p.n, p.span[i], p.sdiv[i], npair, pdiv, ldc, p.tw, tid,
-                                                nthr);
+            fft_stage_pair_dispatch<true, true, false, false, NoEpi, PTW>(p.radix[i], s, p.n, p.span[i], p.sdiv[i],
+                                                                          npair, pdiv, ldc, p.tw, tid, nthr);
         ASARF_SYNC();
     }
 }
@@ -641,31 +641,31 @@ ASARF_HD ASARF_INLINE void fft_inverse_dif_pairs_ct3(float2* s, const float2* __
 // Three-stage forward DIF (fft_forward_pairs) and inverse DIT with epilogue (fft_inverse_pairs)
 // of a compile-time radix schedule R0, R1, R2 over a run-time number of columns: the same
 // stages, twiddles and rounding as the run-time versions.
-template <int R0, int R1, int R2>
+template <int R0, int R1, int R2, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_forward_pairs_cs3(float2* s, int ncol, int ldc, const float2* __restrict__ tw, int tid,
                                                  int nthr) {
     constexpr int N = R0 * R1 * R2;
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
-    fft_stage_pair_cs<R0, false, false, N, N / R0>(s, npair, pdiv, ldc, tw, tid, nthr);
+    fft_stage_pair_cs<R0, false, false, N, N / R0, NoEpi, PTW>(s, npair, pdiv, ldc, tw, tid, nthr);
     ASARF_SYNC();
-    fft_stage_pair_cs<R1, false, false, N, R2>(s, npair, pdiv, ldc, tw, tid, nthr);
+    fft_stage_pair_cs<R1, false, false, N, R2, NoEpi, PTW>(s, npair, pdiv, ldc, tw, tid, nthr);
     ASARF_SYNC();
-    fft_stage_pair_cs<R2, false, false, N, 1>(s, npair, pdiv, ldc, tw, tid, nthr);
+    fft_stage_pair_cs<R2, false, false, N, 1, NoEpi, PTW>(s, npair, pdiv, ldc, tw, tid, nthr);
     ASARF_SYNC();
 }
 
-template <int R0, int R1, int R2, class Epi = NoEpi>
+template <int R0, int R1, int R2, class Epi = NoEpi, bool PTW = false>
 ASARF_HD ASARF_INLINE void fft_inverse_pairs_cs3(float2* s, int ncol, int ldc, const float2* __restrict__ tw, int tid,
                                                  int nthr, const Epi& epi = Epi()) {
     constexpr int N = R0 * R1 * R2;
     const int npair = ncol >> 1;
     const FastDiv pdiv = make_fastdiv(static_cast<unsigned int>(npair));
-    fft_stage_pair_cs<R2, true, true, N, 1>(s, npair, pdiv, ldc, tw, tid, nthr);
+    fft_stage_pair_cs<R2, true, true, N, 1, NoEpi, PTW>(s, npair, pdiv, ldc, tw, tid, nthr);
     ASARF_SYNC();
-    fft_stage_pair_cs<R1, true, true, N, R2>(s, npair, pdiv, ldc, tw, tid, nthr);
+    fft_stage_pair_cs<R1, true, true, N, R2, NoEpi, PTW>(s, npair, pdiv, ldc, tw, tid, nthr);
     ASARF_SYNC();
-    fft_stage_pair_cs<R0, true, true, N, N / R0, Epi>(s, npair, pdiv, ldc, tw, tid, nthr, epi);
+    fft_stage_pair_cs<R0, true, true, N, N / R0, Epi, PTW>(s, npair, pdiv, ldc, tw, tid, nthr, epi);
     ASARF_SYNC();
 }
 
