@@ -773,7 +773,16 @@ ASARF_HD inline void finalize_body(const FinalizeArgs& a) {
 // x < XSize - chirp_samples.  Samples the decoder leaves empty are 0 (ZeroNaNs after the
 // correction, main.cc:245).  The FFT length is any L >= XSize: outputs x < Nk only correlate
 // data samples [x, x + Nc) so they do not depend on L.
-ASARF_HD ASARF_INLINE float2 correct_sample_f(float iv, float qv, const FocusState& st) {
+// The IQ correction constants of a run, copied out of the FocusState into registers before a
+// line's decode loop (read through the state's pointer, they were reloaded for every sample:
+// range compression 1.066 -> 0.996 ms on the ERS scene).
+struct IqCorr {
+    float dc_i, dc_q, gain, rgain, sin_c, cos_c, rcos;
+    ASARF_HD ASARF_INLINE explicit IqCorr(const FocusState& s)
+        : dc_i(s.dc_i), dc_q(s.dc_q), gain(s.gain), rgain(s.rgain), sin_c(s.sin_c), cos_c(s.cos_c), rcos(s.rcos) {}
+};
+
+ASARF_HD ASARF_INLINE float2 correct_sample_f(float iv, float qv, const IqCorr& st) {
     const float i1 = fsub_rn(iv, st.dc_i);
     const float q1 = fsub_rn(qv, st.dc_q);
     // the reference's two IEEE divisions, correctly rounded through the reciprocals
@@ -782,7 +791,7 @@ ASARF_HD ASARF_INLINE float2 correct_sample_f(float iv, float qv, const FocusSta
     return make_float2(i2, q2);
 }
 
-ASARF_HD ASARF_INLINE float2 correct_sample(int iv, int qv, const FocusState& st) {
+ASARF_HD ASARF_INLINE float2 correct_sample(int iv, int qv, const IqCorr& st) {
     return correct_sample_f(static_cast<float>(iv), static_cast<float>(qv), st);
 }
 
@@ -803,7 +812,7 @@ struct LineDecoder {
             len = 0;
         }
     }
-    ASARF_HD ASARF_INLINE float2 operator()(const RangeCompressArgs& a, const FocusState& st, int l) const {
+    ASARF_HD ASARF_INLINE float2 operator()(const RangeCompressArgs& a, const IqCorr& st, int l) const {
         float2 z = make_float2(0.0f, 0.0f);
         const int i = l - off;
         if constexpr (FMT == kRawAsarFbaq4) {
@@ -823,7 +832,7 @@ struct LineDecoder {
 template <int FMT = kRawErsBytes>
 ASARF_HD ASARF_INLINE void range_compress_body(const RangeCompressArgs& a, int y, int tid, int nthr, float2* s,
                                                const uint8_t* raw_line) {
-    const FocusState& st = *a.state;
+    const IqCorr st(*a.state);
     const int L = a.plan.n;
     const LineDecoder<FMT> dec(a, y, raw_line);
     for (int l = tid; l < L; l += nthr) s[l] = dec(a, st, l);
@@ -853,7 +862,7 @@ ASARF_HD ASARF_INLINE void range_compress_ct_body(const RangeCompressArgs& a, in
                                                   const uint8_t* raw_line) {
     constexpr int NTHR = CtSchedule<L>::nthr;
     constexpr int PER = (L + NTHR - 1) / NTHR;
-    const FocusState& st = *a.state;
+    const IqCorr st(*a.state);
     const LineDecoder<FMT> dec(a, y, raw_line);
     ct_phase<NTHR>(
         [&](int t) {
