@@ -76,13 +76,21 @@ def build_emu(out_dir: str | os.PathLike, force: bool = False) -> Path:
     if not force and not _stale(out, deps):
         return out
     out.parent.mkdir(parents=True, exist_ok=True)
+    # compiled under a per-process name and renamed into place, so that test processes
+    # running side by side never load a half-written library
+    tmp = out.with_name(f".{out.name}.{os.getpid()}.tmp")
     cxx = os.environ.get("CXX", "g++")
     cmd = [cxx, "-std=c++17", "-O2", "-ffp-contract=off", "-fno-strict-aliasing", "-fPIC", "-shared", "-DASARF_HOST_EMU",
            f"-I{INC}", f"-I{CSRC}", f"-I{CUDA_INC}", "-x", "c++", str(CSRC / "host.cpp"), "-x", "c++",
            str(CSRC / "stages.cpp"), "-x", "c++", str(CSRC / "batch.cpp"), "-x", "c++", str(CSRC / "strip.cpp"), "-x", "c++",
            str(CSRC / "l0.cpp"), "-x", "c++", str(CSRC / "emu.cpp"),
-           "-o", str(out)]
-    _run(cmd)
+           "-o", str(tmp)]
+    try:
+        _run(cmd)
+        os.replace(tmp, out)
+    finally:
+        if tmp.exists():
+            tmp.unlink()
     return out
 
 
