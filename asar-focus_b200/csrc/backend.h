@@ -59,6 +59,7 @@ int event_record(void* e, void* stream);
 int event_elapsed(void* a, void* b, float* ms);
 int event_sync(void* e);
 size_t smem_optin_limit();
+int backend_sm_count();  // streaming multiprocessors of the current device
 // Streams, cross-stream waits and CUDA graphs (device build).  The host emulation has no
 // graphs: graphs_supported() is false there and callers run their sequence directly.
 void* stream_create();

@@ -112,6 +112,26 @@ constexpr int kStatsMaxLines = 256;
 // lines per block of the statistics kernel (measured on the 28000- and 30000-line scenes:
 // 64 -> 0.203, 128 -> 0.170, 192 -> 0.155, 256 -> 0.171 ms)
 constexpr int kStatsLinesPerBlock = 192;
+constexpr int kStatsBlocksPerSm = 3;  // resident blocks of k_raw_stats (its launch bounds)
+
+// Lines per statistics block for a grid of gx block columns over na lines: kStatsLinesPerBlock,
+// raised in whole batches (at most kStatsMaxLines) when that fits the grid into one wave fewer
+// of the `slots` resident blocks, since the last wave of a grid of equal blocks runs mostly
+// empty (ASAR IM-like 30000 lines, 6 columns, 444 slots: 942 blocks of 192 lines take three
+// waves, 870 of 208 lines two).
+inline int stats_lines_per_block(int na, int gx, int slots) {
+    const long long rows = (na + kStatsLinesPerBlock - 1) / kStatsLinesPerBlock;
+    const long long waves = (rows * gx + slots - 1) / slots;
+    if (waves > 1 && gx > 0) {
+        const long long fit_rows = (waves - 1) * slots / gx;
+        if (fit_rows > 0) {
+            long long l = (na + fit_rows - 1) / fit_rows;
+            l = (l + kStatsBatch - 1) / kStatsBatch * kStatsBatch;
+            if (l <= kStatsMaxLines) return static_cast<int>(l);
+        }
+    }
+    return kStatsLinesPerBlock;
+}
 
 struct RawStatsSmem {
     unsigned long long mom[6];

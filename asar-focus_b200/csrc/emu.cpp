@@ -231,6 +231,7 @@ int event_elapsed(void*, void*, float* ms) {
     return ASARF_OK;
 }
 size_t smem_optin_limit() { return 227 * 1024; }
+int backend_sm_count() { return 148; }  // the B200's, so plans take the device build's shapes
 
 }  // namespace asarf
 

@@ -842,8 +842,15 @@ int asarf_plan_create(const asarf_scene* scene, const asarf_options* opt_in, asa
     st.nr = p->nr;
     st.dc_step = dc_step;
     st.nblk = nblk;
-    st.lines_per_cta = kStatsLinesPerBlock;
     st.acc = p->acc;
+    {
+        // block height for the grid of aligned raw buffers (the 4-column path, any address
+        // that is a multiple of 8: a null pointer stands for one); an unaligned buffer runs
+        // the one-column path over the same lines
+        RawStatsArgs shape = st;
+        const int gx = raw_stats_grid_x(shape, nullptr);
+        st.lines_per_cta = stats_lines_per_block(p->na, gx, backend_sm_count() * kStatsBlocksPerSm);
+    }
     p->stats_gy = (p->na + st.lines_per_cta - 1) / st.lines_per_cta;
     if (fbaq) {
         st.lut_i = lut_dev;
